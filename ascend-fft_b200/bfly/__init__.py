@@ -1,0 +1,21 @@
+"""bfly: batched power-of-two fp32 FFTs on NVIDIA B200 (sm_100a).
+
+A drop-in for the plan API of TruNcat3/ascend-fft (Context.init(profile, space, kernel),
+select / make_plan, Plan.run / run_r2c / run_c2r / measure) plus asynchronous device-pointer
+entry points and torch.fft-style functions with autograd.  All transforms run in the
+hand-written CUDA kernels of libbfly_b200.so; importing the transforms without the built
+library raises.
+"""
+from ._lib import LIB_PATH, load
+from .core import (DEFAULT_CANDIDATE, DEFAULT_PROFILE, DEFAULT_SPACE, BflyError, Context, Plan)
+
+__all__ = ["LIB_PATH", "load", "Context", "Plan", "BflyError", "DEFAULT_PROFILE", "DEFAULT_SPACE",
+           "DEFAULT_CANDIDATE", "fft", "ifft", "rfft", "irfft", "c2c", "r2c", "c2r", "plan_for"]
+
+
+def __getattr__(name):
+    # torch-level ops are imported lazily so the plan API works without importing torch.
+    if name in ("fft", "ifft", "rfft", "irfft", "c2c", "r2c", "c2r", "plan_for"):
+        from . import ops
+        return getattr(ops, name)
+    raise AttributeError(name)

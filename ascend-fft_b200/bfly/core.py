@@ -1,0 +1,171 @@
+"""Python mirror of the reference's plan API: Context.init(profile, space, kernel), select,
+enumerate, make_plan, and Plan.prepare / run / run_r2c / run_c2r / measure with the reference's
+integer status codes (TruNcat3/ascend-fft include/butterfly/plan.hpp:26-91).  Host-pointer
+calls take numpy float32 arrays; exec_* calls take device pointers (ints) and a CUDA stream
+handle and return immediately.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+
+PKG_ROOT = Path(__file__).resolve().parents[1]
+DEFAULT_PROFILE = PKG_ROOT / "config" / "b200_profile.json"
+DEFAULT_SPACE = PKG_ROOT / "config" / "b200_space.json"
+DEFAULT_CANDIDATE = "r16_cta256_shared_fp32_stockham"
+
+STATUS = {0: "ok", -1: "kernel unavailable / runtime", -2: "prepare / device", -3: "alloc / stream",
+          -4: "H2D / configuration", -5: "launch", -6: "sync", -7: "D2H / acceptance",
+          -8: "shape or guard", -9: "already initialised", -10: "null argument",
+          -11: "buffer too small"}
+
+
+class BflyError(RuntimeError):
+    def __init__(self, what: str, code: int):
+        super().__init__(f"{what} failed with status {code} ({STATUS.get(code, '?')})")
+        self.code = code
+
+
+def _check(what: str, code: int) -> int:
+    if code != 0:
+        raise BflyError(what, code)
+    return code
+
+
+def _ptr(a: np.ndarray) -> int:
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data
+
+
+class Context:
+    """bfly::Context over the C ABI.  init() returns the reference's status code."""
+
+    def __init__(self):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        _check("bfly_context_create", self._lib.bfly_context_create(C.byref(h)))
+        self._h = h
+
+    def init(self, profile=DEFAULT_PROFILE, space=DEFAULT_SPACE, kernel="builtin", device=None) -> int:
+        args = (self._h, str(profile).encode(), str(space).encode(), str(kernel).encode())
+        if device is None:
+            return self._lib.bfly_context_init(*args)
+        return self._lib.bfly_context_init_device(*args, int(device))
+
+    def enumerate(self, n: int, batch: int):
+        need = C.c_size_t(0)
+        cnt = C.c_int(0)
+        self._lib.bfly_context_enumerate(self._h, n, batch, None, 0, C.byref(cnt), C.byref(need))
+        buf = C.create_string_buffer(need.value + 1)
+        _check("enumerate", self._lib.bfly_context_enumerate(self._h, n, batch, buf, len(buf),
+                                                               C.byref(cnt), C.byref(need)))
+        out = []
+        for line in buf.value.decode().splitlines():
+            cid, state, reason = (line.split("\t") + ["", ""])[:3]
+            out.append({"id": cid, "state": state, "reason": reason})
+        return out
+
+    def select(self, n: int, batch: int, top_k: int = 3, want_log: bool = False):
+        p = C.c_void_p()
+        log = C.create_string_buffer(1 << 16) if want_log else None
+        rc = self._lib.bfly_context_select(self._h, n, batch, top_k, C.byref(p), log,
+                                           len(log) if log is not None else 0)
+        plan = Plan(self, p) if rc == 0 else None
+        return (plan, log.value.decode() if log is not None else "") if want_log else plan
+
+    def make_plan(self, candidate_id: str = DEFAULT_CANDIDATE, n: int = 1024, batch: int = 1):
+        p = C.c_void_p()
+        rc = self._lib.bfly_context_make_plan(self._h, n, batch, candidate_id.encode(), C.byref(p))
+        return Plan(self, p) if rc == 0 else None
+
+    def set_tuning_cache(self, path) -> None:
+        self._lib.bfly_context_set_tuning_cache(self._h, str(path).encode() if path else b"")
+
+    @property
+    def stream(self) -> int:
+        return self._lib.bfly_context_stream(self._h) or 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bfly_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """bfly::Plan over the C ABI.  Methods return the reference's status codes."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p):
+        self._ctx = ctx   # keeps the context (and its stream) alive
+        self._lib = ctx._lib
+        self._h = handle
+
+    @property
+    def candidate_id(self) -> str:
+        buf = C.create_string_buffer(256)
+        self._lib.bfly_plan_candidate_id(self._h, buf, len(buf))
+        return buf.value.decode()
+
+    def prepare(self, n: int, batch: int = 0xFFFFFFFF) -> int:
+        return self._lib.bfly_plan_prepare(self._h, n, batch)
+
+    # ---- synchronous host-pointer API (numpy float32 buffers)
+    def run(self, x: np.ndarray, out: np.ndarray, n: int, batch: int) -> int:
+        return self._lib.bfly_plan_run_c2c(self._h, _ptr(x), _ptr(out), n, batch)
+
+    def run_r2c(self, x: np.ndarray, out: np.ndarray, n: int, batch: int) -> int:
+        return self._lib.bfly_plan_run_r2c(self._h, _ptr(x), _ptr(out), n, batch)
+
+    def run_c2r(self, x: np.ndarray, out: np.ndarray, n: int, batch: int) -> int:
+        return self._lib.bfly_plan_run_c2r(self._h, _ptr(x), _ptr(out), n, batch)
+
+    def run_inverse(self, x: np.ndarray, out: np.ndarray, n: int, batch: int, scale: float = 1.0) -> int:
+        return self._lib.bfly_plan_run_c2c_inverse(self._h, _ptr(x), _ptr(out), n, batch, scale)
+
+    def run_long(self, x: np.ndarray, out: np.ndarray, n: int, batch: int, direction: int = -1) -> int:
+        return self._lib.bfly_plan_run_c2c_long(self._h, _ptr(x), _ptr(out), n, batch, direction)
+
+    def measure(self, n: int, batch: int):
+        m = _lib.Metric()
+        rc = self._lib.bfly_plan_measure(self._h, n, batch, C.byref(m))
+        return rc, {"eta_us": m.eta_us, "measured_us": m.measured_us,
+                    "max_rel_err": m.max_rel_err, "measured_ok": bool(m.measured_ok)}
+
+    # ---- asynchronous device-pointer API
+    def exec_c2c(self, d_in: int, d_out: int, n: int, batch: int, direction: int = -1,
+                 scale: float = 1.0, stream: int = 0) -> int:
+        return self._lib.bfly_plan_exec_c2c_async(self._h, d_in, d_out, n, batch, direction,
+                                                  scale, stream or None)
+
+    def exec_r2c(self, d_in: int, d_out: int, n: int, batch: int, s_edge: float = 1.0,
+                 s_int: float = 1.0, stream: int = 0) -> int:
+        return self._lib.bfly_plan_exec_r2c_async(self._h, d_in, d_out, n, batch, s_edge, s_int,
+                                                  stream or None)
+
+    def exec_c2r(self, d_in: int, d_out: int, n: int, batch: int, s_edge: float = 1.0,
+                 s_int: float = 1.0, out_scale: float | None = None, stream: int = 0) -> int:
+        if out_scale is None:
+            out_scale = 1.0 / n
+        return self._lib.bfly_plan_exec_c2r_async(self._h, d_in, d_out, n, batch, s_edge, s_int,
+                                                  out_scale, stream or None)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bfly_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,68 @@
+// Device seam of the host runtime.  plan.cpp (Context / Plan / autotuner) is plain C++ and
+// reaches the GPU only through these functions; backend_cuda.cu implements them on the CUDA
+// runtime and the hand-written sm_100a kernels, and the CPU guard tests link a counting fake
+// with failure injection instead (the pattern of the reference's tests/stubs/acl/acl_rt.h:15-53).
+// Every function returns 0 on success and a nonzero CUDA-style error otherwise.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace bfly {
+namespace backend {
+
+// ------------------------------------------------------------------ runtime
+int deviceCount(int* count);
+int setDevice(int device);
+int deviceName(int device, char* buf, size_t cap);
+int smCount(int device, int* count);
+int streamCreate(void** stream);
+int streamDestroy(void* stream);
+int alloc(void** ptr, size_t bytes);
+int release(void* ptr);
+int allocHost(void** ptr, size_t bytes);   // pinned staging buffer
+int releaseHost(void* ptr);
+int copyH2D(void* dst, const void* src, size_t bytes, void* stream);
+int copyD2H(void* dst, const void* src, size_t bytes, void* stream);
+int streamSync(void* stream);
+
+// Device-side elapsed time between start() and stop() on one stream (CUDA events).
+struct Timer;
+int timerCreate(Timer** timer);
+int timerStart(Timer* timer, void* stream);
+int timerStop(Timer* timer, void* stream, float* ms);   // synchronises the stop event
+void timerDestroy(Timer* timer);
+
+// ------------------------------------------------------------------ kernel variants
+// kind: which kernel family; n: transform length (real length for R2C/C2R);
+// e: complex values per thread (register radix); cta: threads per CTA.
+enum Kind : int { kC2C = 0, kR2C = 1, kC2R = 2 };
+bool hasVariant(int kind, uint32_t n, int e, int cta);
+size_t variantSmemBytes(int kind, uint32_t n, int e, int cta);
+
+// Twiddle tables (float2 entries), all computed in FP64 on the device.
+size_t stockhamTwiddleCount(uint32_t n, int e);        // Sched<n,e>::TWSIZE (0 if none)
+int buildStockhamTwiddles(void* tw, uint32_t n, int e, void* stream);
+// tw[i] = exp(-2*pi*i*(i*stride mod n)/n), i < count
+int buildLinearTwiddles(void* tw, int count, long long stride, long long n, void* stream);
+
+int launchC2C(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+              const void* tw, int e, int cta, void* stream);
+// R2C of real length n: tw = Stockham table of (n/2, e), twr = W_n^k for k = 0..n/2.
+int launchR2C(const void* in, void* out, uint32_t n, uint64_t batch, const void* tw,
+              const void* twr, int e, int cta, bool weighted, float sEdge, float sInt,
+              void* stream);
+int launchC2R(const void* in, void* out, uint32_t n, uint64_t batch, const void* tw,
+              const void* twr, int e, int cta, float sEdge, float sInt, float outScale,
+              void* stream);
+
+// Four-step long C2C, n = n1 * n2.
+bool hasLongSplit(uint32_t n1, uint32_t n2);
+void longSplit(uint32_t n, uint32_t* n1, uint32_t* n2);   // chosen split (0,0 if none)
+int longE();                                                // register radix of both passes
+int launchLongA(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t batch,
+                bool inverse, const void* tw1, const void* tlo, const void* thi, void* stream);
+int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t batch,
+                bool inverse, float scale, const void* tw2, void* stream);
+
+}  // namespace backend
+}  // namespace bfly

@@ -1,0 +1,907 @@
+// Host runtime of the batched FFT library: configuration loading, candidate enumeration,
+// the measuring autotuner with a persisted choice cache, and the Plan entry points.
+// Reference behaviour mirrored (TruNcat3/ascend-fft):
+//   Hardware::load / DesignSpace::load   src/framework/butterfly.cpp:71-93, 326-350
+//   enumerate / rank                     butterfly.cpp:383-512
+//   Plan::prepare / run / runR2C / runC2R / measure   butterfly.cpp:587-924
+//   Context::init / makePlan / select    butterfly.cpp:938-1102
+// Status codes and the "guards before any allocation" rule follow the reference's
+// docs/reference/api.md:34-50 and tests/test_runtime_guards.cpp:139-159.
+// This file is plain C++: the GPU is reached only through backend.h.
+#include "bfly/plan.hpp"
+
+#include "backend.h"
+#include "json_config.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <utility>
+
+namespace bfly {
+
+namespace {
+
+constexpr uint32_t kMinN = 32;        // two passes of radix <= 16
+constexpr uint32_t kMaxSinglePass = 16384;
+constexpr uint32_t kMaxN = 65536;
+
+std::string slurp(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw std::runtime_error("cannot read configuration: " + path);
+    return std::string(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+}
+
+bool pow2(uint64_t v) { return v && !(v & (v - 1)); }
+
+int positiveInt(const json::Node& root, const char* key) {
+    const long long v = root.get(key).asInt();
+    if (v <= 0 || v > 0x7fffffffLL) throw std::runtime_error(std::string(key) + " must be a positive int");
+    return (int)v;
+}
+
+const std::vector<json::Node>& axis(const json::Node& obj, const char* key) {
+    const json::Node& v = obj.get(key);
+    if (v.kind != json::Node::Array || v.items.empty())
+        throw std::runtime_error(std::string(key) + " must be a nonempty array");
+    return v.items;
+}
+
+void intAxis(const json::Node& obj, const char* key, std::vector<int>* out, int lo, int hi) {
+    out->clear();
+    for (const auto& v : axis(obj, key)) {
+        const long long x = v.asInt();
+        if (x < lo || x > hi) throw std::runtime_error(std::string(key) + " contains an invalid value");
+        out->push_back((int)x);
+    }
+}
+
+void stringAxis(const json::Node& obj, const char* key, std::vector<std::string>* out,
+                std::initializer_list<const char*> allowed) {
+    out->clear();
+    for (const auto& v : axis(obj, key)) {
+        const std::string& s = v.asString();
+        bool ok = false;
+        for (const char* a : allowed) ok = ok || s == a;
+        if (!ok) throw std::runtime_error(std::string(key) + " contains unsupported value " + s);
+        out->push_back(s);
+    }
+}
+
+enum ShapeKind { kRunC2C, kRunR2C, kRunC2R, kRunLong, kPrepare, kMeasure, kExecC2C, kExecR2C, kExecC2R };
+
+// Real transforms run an n/2-point complex FFT.
+constexpr uint32_t kRealMin = 64, kRealMax = 8192;
+
+}  // namespace
+
+// ================================================================== H
+Hardware Hardware::load(const std::string& path) {
+    const json::Node root = json::parse(slurp(path));
+    if (root.get("schema_version").asInt() != 1)
+        throw std::runtime_error("unsupported hardware schema_version");
+    Hardware hw;
+    hw.gpu = root.get("gpu").asString();
+    hw.arch = root.get("arch").asString();
+    if (root.has("device_index")) {
+        const long long d = root.get("device_index").asInt();
+        if (d < 0 || d > 1024) throw std::runtime_error("device_index out of range");
+        hw.deviceIndex = (int)d;
+    }
+    hw.smCount = positiveInt(root, "sm_count");
+    hw.smemPerCta = positiveInt(root, "smem_bytes_per_cta");
+    hw.smemPerSm = positiveInt(root, "smem_bytes_per_sm");
+    hw.regsPerSm = positiveInt(root, "regs_per_sm");
+    hw.maxThreadsPerSm = positiveInt(root, "max_threads_per_sm");
+    if (root.has("l2_bytes")) {
+        hw.l2Bytes = root.get("l2_bytes").asInt();
+        if (hw.l2Bytes < 0) throw std::runtime_error("l2_bytes must be >= 0");
+    }
+    hw.hbmGbs = root.get("hbm_gbs").asDouble();
+    if (!(hw.hbmGbs > 0.0) || hw.smemPerCta > hw.smemPerSm)
+        throw std::runtime_error("hardware configuration contains nonpositive or inconsistent resources");
+    return hw;
+}
+
+// ================================================================== A / P
+bool Mapping::validate(const Hardware& hw, std::string* why) const {
+    auto fail = [&](const char* m) {
+        if (why) *why = m;
+        return false;
+    };
+    if (ctaThreads <= 0) return fail("cta_threads must be > 0");
+    if (ctaThreads > 1024 || ctaThreads % 32) return fail("cta_threads must be a multiple of 32 in [32, 1024]");
+    if (hw.maxThreadsPerSm > 0 && ctaThreads > hw.maxThreadsPerSm) return fail("cta_threads exceeds max_threads_per_sm");
+    if (level != 0) return fail("level!=0 (multi-GPU) is batch sharding above the plan, not a plan mapping");
+    if (localExchange == "shuffle")
+        return fail("local_exchange=shuffle is not lowered (passes exchange through shared memory)");
+    if (localExchange != "shared") return fail("unknown local_exchange");
+    return true;
+}
+
+size_t StagePlan::smemBytes(uint32_t n, int ctaThreads) const {
+    if (radix <= 0 || n < (uint32_t)radix) return 0;
+    const uint32_t T = n / (uint32_t)radix;
+    if (!T || (uint32_t)ctaThreads < T) return 0;
+    const uint32_t rows = (uint32_t)ctaThreads / T;
+    uint32_t stride = (n - 1) + ((n - 1) >> 4) + 1;   // one pad word per 16
+    if (T < 16) stride += ((T - stride % 16) % 16 + 16) % 16;
+    return (size_t)rows * stride * 8u;
+}
+
+// ================================================================== space
+DesignSpace DesignSpace::load(const std::string& path) {
+    DesignSpace sp;
+    sp.raw = slurp(path);
+    const json::Node root = json::parse(sp.raw);
+    if (root.get("schema_version").asInt() != 1)
+        throw std::runtime_error("unsupported design-space schema_version");
+    const json::Node& a = root.get("A");
+    const json::Node& p = root.get("P");
+    const json::Node& l = root.get("L");
+    const json::Node& f = root.get("F");
+    intAxis(a, "cta_threads", &sp.ctaThreads, 1, 1024);
+    for (int c : sp.ctaThreads)
+        if (c % 32) throw std::runtime_error("cta_threads must be multiples of 32");
+    stringAxis(a, "local_exchange", &sp.localExchanges, {"shared", "shuffle"});
+    intAxis(p, "radix", &sp.radices, 2, 16);
+    for (int r : sp.radices)
+        if (r != 2 && r != 4 && r != 8 && r != 16) throw std::runtime_error("radix must be 2, 4, 8 or 16");
+    intAxis(p, "fusion_level", &sp.fusionStages, 1, 24);
+    sp.coeffResidency.clear();
+    for (const auto& v : axis(p, "coefficient_residency")) sp.coeffResidency.push_back(v.asBool() ? 1 : 0);
+    stringAxis(l, "in", &sp.layoutsIn, {"interleaved", "planar"});
+    stringAxis(l, "out", &sp.layoutsOut, {"interleaved", "planar"});
+    stringAxis(f, "precision", &sp.precisions, {"fp32", "split_bf16"});
+    stringAxis(f, "schedule", &sp.schedules, {"stockham", "four_step"});
+    return sp;
+}
+
+void DesignSpace::applyDefaults() {
+    if (ctaThreads.empty()) ctaThreads = {128, 256, 512};
+    if (radices.empty()) radices = {8, 16};
+    if (fusionStages.empty()) fusionStages = {1};
+    if (coeffResidency.empty()) coeffResidency = {1};
+    if (localExchanges.empty()) localExchanges = {"shared"};
+    if (layoutsIn.empty()) layoutsIn = {"interleaved"};
+    if (layoutsOut.empty()) layoutsOut = {"interleaved"};
+    if (precisions.empty()) precisions = {"fp32"};
+    if (schedules.empty()) schedules = {"stockham", "four_step"};
+}
+
+const char* toString(State s) {
+    switch (s) {
+        case State::Infeasible: return "Infeasible";
+        case State::Unverified: return "Unverified";
+        case State::Feasible: return "Feasible";
+        case State::Measured: return "Measured";
+    }
+    return "?";
+}
+
+// ================================================================== estimate
+// Roofline estimate: compulsory HBM bytes at the profile's measured bandwidth, a fixed launch
+// cost, a per-extra-pass smem term, and a second HBM round trip for the four-step schedule.
+Metric estimate(const Hardware& hw, const Candidate& c, uint32_t n, uint32_t batch) {
+    Metric m;
+    if (!n || !batch || hw.hbmGbs <= 0) return m;
+    const double bytes = 16.0 * (double)n * (double)batch;
+    const double hbmUs = bytes / (hw.hbmGbs * 1e3);
+    int logn = 0;
+    while ((1u << logn) < n) ++logn;
+    int loge = 0;
+    while (c.p.radix > 1 && (1 << loge) < c.p.radix) ++loge;
+    const int passes = loge ? (logn + loge - 1) / loge : logn;
+    double us = 2.5 + hbmUs * (1.0 + 0.04 * std::max(0, passes - 2));
+    if (c.f.schedule == "four_step") us = 3.0 + 2.0 * hbmUs;
+    if (c.a.ctaThreads < 256) us *= 1.02;
+    m.etaUs = us;
+    return m;
+}
+
+// ================================================================== enumerate
+std::vector<Candidate> enumerate(const DesignSpace& sp, const Hardware& hw, uint32_t n,
+                                 uint32_t batch) {
+    std::vector<Candidate> out;
+    auto pack = [](const std::string& s) { return s == "planar" ? Layout::Planar : Layout::Interleaved; };
+    char buf[256];
+    for (int cta : sp.ctaThreads)
+      for (int radix : sp.radices)
+        for (int fl : sp.fusionStages)
+          for (int cr : sp.coeffResidency)
+            for (const std::string& lx : sp.localExchanges)
+              for (const std::string& li : sp.layoutsIn)
+                for (const std::string& lo : sp.layoutsOut)
+                  for (const std::string& prec : sp.precisions)
+                    for (const std::string& sched : sp.schedules) {
+        Candidate c;
+        c.a.ctaThreads = cta;
+        c.a.localExchange = lx;
+        c.p.radix = radix;
+        c.p.fusionLevel = fl;
+        c.p.coefficientResidency = cr != 0;
+        c.l.in = pack(li);
+        c.l.out = pack(lo);
+        c.f.precision = prec;
+        c.f.schedule = sched;
+        std::snprintf(buf, sizeof(buf), "r%d_cta%d_%s_%s_%s", radix, cta, lx.c_str(), prec.c_str(), sched.c_str());
+        c.id = buf;
+        if (fl != 1) c.id += "_f" + std::to_string(fl);
+        if (c.l.in == Layout::Planar) c.id += "_inplanar";
+        if (c.l.out == Layout::Planar) c.id += "_outplanar";
+        if (!c.p.coefficientResidency) c.id += "_noRes";
+
+        auto infeasible = [&](const std::string& why) {
+            c.state = State::Infeasible;
+            c.reason = why;
+        };
+        std::string why;
+        const uint32_t T = radix > 0 ? n / (uint32_t)radix : 0;
+        if (!c.a.validate(hw, &why)) {
+            infeasible(why);
+        } else if (!c.p.coefficientResidency) {
+            infeasible("kernels read twiddle tables through L1; coefficient_residency=false is not lowered");
+        } else if (!pow2(n)) {
+            infeasible("n must be a power of two");
+        } else if (n < kMinN) {
+            infeasible("n below the 32-point minimum (two passes of radix <= 16)");
+        } else if (n > kMaxN) {
+            infeasible("n exceeds the 65536-point envelope");
+        } else if (batch == 0) {
+            infeasible("batch must be positive");
+        } else if ((uint64_t)batch * 2ull * n > 0xFFFFFFFFull) {
+            std::snprintf(buf, sizeof(buf),
+                          "batch*2*n = %llu exceeds the uint32 element offsets of the host-pointer API "
+                          "(max batch for n=%u is %llu)",
+                          (unsigned long long)batch * 2ull * n, n,
+                          (unsigned long long)(0xFFFFFFFFull / (2ull * n)));
+            infeasible(buf);
+        } else if (c.l.in != Layout::Interleaved || c.l.out != Layout::Interleaved) {
+            infeasible("planar layout is not lowered (kernels consume and produce interleaved fp32)");
+        } else if (fl != 1) {
+            infeasible("fusion_level!=1 is not lowered (each schedule fuses all of its passes)");
+        } else if (prec != "fp32") {
+            infeasible("split_bf16 is served by the tensor-core entry points, not by plan candidates");
+        } else if (sched == "four_step") {
+            uint32_t n1 = 0, n2 = 0;
+            backend::longSplit(n, &n1, &n2);
+            if (n <= 4096) infeasible("four_step is only used for n > 4096");
+            else if (!n1 || !backend::hasLongSplit(n1, n2)) infeasible("no four-step split for this n");
+            else if (radix != backend::longE() || cta != 256)
+                infeasible("four_step kernels use radix 16 and 256-thread CTAs");
+            else c.state = State::Unverified;
+        } else {   // stockham single pass
+            const size_t smem = c.p.smemBytes(n, cta);
+            if (n > kMaxSinglePass) {
+                infeasible("single-pass stockham holds at most 16384 points in shared memory");
+            } else if ((uint32_t)radix > n / 2) {
+                infeasible("radix must leave at least two passes (radix <= n/2)");
+            } else if (T > (uint32_t)cta || (uint32_t)cta % T) {
+                std::snprintf(buf, sizeof(buf), "n/radix = %u threads per transform do not tile cta_threads=%d", T, cta);
+                infeasible(buf);
+            } else if (smem > (size_t)hw.smemPerCta) {
+                std::snprintf(buf, sizeof(buf), "shared memory %.1f KiB > %d KiB per CTA (radix=%d, n=%u)",
+                              smem / 1024.0, hw.smemPerCta / 1024, radix, n);
+                infeasible(buf);
+            } else if (!backend::hasVariant(backend::kC2C, n, radix, cta)) {
+                std::snprintf(buf, sizeof(buf), "no compiled kernel for (n=%u, radix=%d, cta=%d)", n, radix, cta);
+                infeasible(buf);
+            } else {
+                c.state = State::Unverified;
+            }
+        }
+        c.q = estimate(hw, c, n, batch);
+        out.push_back(std::move(c));
+    }
+    return out;
+}
+
+std::vector<const Candidate*> rank(const std::vector<Candidate>& cs) {
+    std::vector<const Candidate*> v;
+    for (const auto& c : cs)
+        if (c.state != State::Infeasible) v.push_back(&c);
+    std::stable_sort(v.begin(), v.end(), [](const Candidate* x, const Candidate* y) {
+        if (x->state != y->state) return x->state > y->state;
+        return x->q.etaUs < y->q.etaUs;
+    });
+    return v;
+}
+
+// A candidate the kernels can execute (independent of n).
+static bool lowerable(const Candidate& c, const Hardware& hw) {
+    return c.a.validate(hw, nullptr) && c.p.coefficientResidency && c.p.fusionLevel == 1 &&
+           (c.p.radix == 8 || c.p.radix == 16) && c.l.contiguous &&
+           c.l.in == Layout::Interleaved && c.l.out == Layout::Interleaved &&
+           c.f.precision == "fp32" && (c.f.schedule == "stockham" || c.f.schedule == "four_step") &&
+           (c.a.ctaThreads == 128 || c.a.ctaThreads == 256 || c.a.ctaThreads == 512 ||
+            c.a.ctaThreads == 1024);
+}
+
+// ================================================================== Plan
+struct Plan::Impl {
+    Hardware hw;
+    int device = 0;
+    std::map<std::pair<uint32_t, int>, void*> twC2C;   // (n, e) -> Stockham table
+    std::map<uint32_t, void*> twReal;                  // n -> W_n^k, k <= n/2
+    struct LongTw {
+        void* lo = nullptr;
+        void* hi = nullptr;
+    };
+    std::map<uint32_t, LongTw> twLong;                 // n -> two-level W_n tables
+    void* devIn = nullptr;
+    void* devOut = nullptr;
+    void* devWork = nullptr;
+    size_t devInCap = 0, devOutCap = 0, devWorkCap = 0;
+    backend::Timer* timer = nullptr;
+};
+
+Plan::Plan(Candidate c) : cand_(std::move(c)) {}
+
+Plan::~Plan() {
+    if (!impl_) return;
+    for (auto& kv : impl_->twC2C) if (kv.second) backend::release(kv.second);
+    for (auto& kv : impl_->twReal) if (kv.second) backend::release(kv.second);
+    for (auto& kv : impl_->twLong) {
+        if (kv.second.lo) backend::release(kv.second.lo);
+        if (kv.second.hi) backend::release(kv.second.hi);
+    }
+    if (impl_->devIn) backend::release(impl_->devIn);
+    if (impl_->devOut) backend::release(impl_->devOut);
+    if (impl_->devWork) backend::release(impl_->devWork);
+    backend::timerDestroy(impl_->timer);
+}
+
+static int ensureBuf(void** p, size_t* cap, size_t bytes) {
+    if (*cap >= bytes && *p) return 0;
+    if (*p) {
+        backend::release(*p);
+        *p = nullptr;
+    }
+    *cap = 0;
+    if (backend::alloc(p, bytes)) {
+        *p = nullptr;
+        return -1;
+    }
+    *cap = bytes;
+    return 0;
+}
+
+bool Plan::validShape(uint32_t n, uint32_t batch, int kind) const {
+    if (!impl_ || batch == 0 || !pow2(n)) return false;
+    const bool offsetGuard = kind == kRunC2C || kind == kRunR2C || kind == kRunC2R ||
+                             kind == kRunLong || kind == kMeasure;
+    switch (kind) {
+        case kRunC2C: if (n < 64 || n > 4096) return false; break;
+        case kRunR2C: if (n < 128 || n > 8192) return false; break;
+        case kRunC2R: if (n < 64 || n > 4096) return false; break;
+        case kRunLong: if (n < 8192 || n > kMaxN) return false; break;
+        case kPrepare:
+        case kMeasure:
+        case kExecC2C: if (n < kMinN || n > kMaxN) return false; break;
+        case kExecR2C:
+        case kExecC2R: if (n < kRealMin || n > kRealMax) return false; break;
+        default: return false;
+    }
+    if (offsetGuard && (uint64_t)batch * 2ull * n > 0xFFFFFFFFull) return false;
+    int e = 0, cta = 0;
+    const int rk = (kind == kRunR2C || kind == kExecR2C) ? backend::kR2C
+                 : (kind == kRunC2R || kind == kExecC2R) ? backend::kC2R : backend::kC2C;
+    return resolve(rk, n, &e, &cta) == 0;
+}
+
+// Kernel variant for (kind, n): the candidate's radix/cta when compiled for n; C2C lengths past
+// the single-pass envelope (or candidates scheduled four_step) use the four-step kernels
+// (reported as e = 0).
+int Plan::resolve(int kind, uint32_t n, int* e, int* cta) const {
+    const int r = cand_.p.radix, c = cand_.a.ctaThreads;
+    if (kind == backend::kC2C) {
+        const bool wantLong = cand_.f.schedule == "four_step" || n > kMaxSinglePass ||
+                              !backend::hasVariant(backend::kC2C, n, r, c);
+        if (!wantLong) {
+            *e = r;
+            *cta = c;
+            return 0;
+        }
+        uint32_t n1 = 0, n2 = 0;
+        backend::longSplit(n, &n1, &n2);
+        if (n1 && backend::hasLongSplit(n1, n2)) {
+            *e = 0;
+            *cta = 256;
+            return 0;
+        }
+        return -1;
+    }
+    if (!backend::hasVariant(kind, n, r, c)) return -1;
+    *e = r;
+    *cta = c;
+    return 0;
+}
+
+int Plan::prepareC2C(uint32_t n, int e) {
+    const auto key = std::make_pair(n, e);
+    if (impl_->twC2C.count(key)) return 0;
+    const size_t count = backend::stockhamTwiddleCount(n, e);
+    void* tw = nullptr;
+    if (count) {
+        if (backend::alloc(&tw, count * 8)) return -1;
+        if (backend::buildStockhamTwiddles(tw, n, e, stream_) || backend::streamSync(stream_)) {
+            backend::release(tw);
+            return -1;
+        }
+    }
+    impl_->twC2C[key] = tw;
+    return 0;
+}
+
+int Plan::prepareReal(uint32_t n) {
+    if (impl_->twReal.count(n)) return 0;
+    void* tw = nullptr;
+    const int count = (int)(n / 2 + 1);
+    if (backend::alloc(&tw, (size_t)count * 8)) return -1;
+    if (backend::buildLinearTwiddles(tw, count, 1, n, stream_) || backend::streamSync(stream_)) {
+        backend::release(tw);
+        return -1;
+    }
+    impl_->twReal[n] = tw;
+    return 0;
+}
+
+int Plan::prepareLong(uint32_t n) {
+    uint32_t n1 = 0, n2 = 0;
+    backend::longSplit(n, &n1, &n2);
+    if (!n1) return -1;
+    if (prepareC2C(n1, backend::longE()) || prepareC2C(n2, backend::longE())) return -1;
+    if (impl_->twLong.count(n)) return 0;
+    Impl::LongTw t;
+    const int nhi = (int)(n / 256);
+    if (backend::alloc(&t.lo, 256 * 8)) return -1;
+    if (backend::alloc(&t.hi, (size_t)nhi * 8)) {
+        backend::release(t.lo);
+        return -1;
+    }
+    if (backend::buildLinearTwiddles(t.lo, 256, 1, n, stream_) ||
+        backend::buildLinearTwiddles(t.hi, nhi, 256, n, stream_) || backend::streamSync(stream_)) {
+        backend::release(t.lo);
+        backend::release(t.hi);
+        return -1;
+    }
+    impl_->twLong[n] = t;
+    return 0;
+}
+
+int Plan::prepare(uint32_t n, uint32_t batch) {
+    if (!validShape(n, batch, kPrepare)) return -8;
+    int e = 0, cta = 0;
+    if (resolve(backend::kC2C, n, &e, &cta)) return -8;
+    const int rcode = e ? prepareC2C(n, e) : prepareLong(n);
+    if (rcode) return -1;
+    tf_.clear();
+    tf_.push_back({Transform::GenTwiddles, "FP64 twiddle tables built on the device, rounded to fp32"});
+    tf_.push_back({Transform::LaunchKernel, e ? "stockham single-pass kernel on the context stream"
+                                              : "four-step column + row kernels on the context stream"});
+    return 0;
+}
+
+int Plan::execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
+                  float scale, void* stream) {
+    if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull || (direction != -1 && direction != 1))
+        return -8;
+    if (!validShape(n, (uint32_t)batch, kExecC2C)) return -8;
+    void* s = stream ? stream : stream_;
+    const bool inv = direction > 0;
+    int e = 0, cta = 0;
+    resolve(backend::kC2C, n, &e, &cta);
+    if (e) {
+        if (prepareC2C(n, e)) return -2;
+        if (backend::launchC2C(dIn, dOut, n, batch, inv, scale, impl_->twC2C[{n, e}], e, cta, s)) return -5;
+        return 0;
+    }
+    if (prepareLong(n)) return -2;
+    uint32_t n1 = 0, n2 = 0;
+    backend::longSplit(n, &n1, &n2);
+    if (ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
+    const auto& lt = impl_->twLong[n];
+    const int E = backend::longE();
+    if (backend::launchLongA(dIn, impl_->devWork, n1, n2, batch, inv, impl_->twC2C[{n1, E}], lt.lo, lt.hi, s))
+        return -5;
+    if (backend::launchLongB(impl_->devWork, dOut, n1, n2, batch, inv, scale, impl_->twC2C[{n2, E}], s))
+        return -5;
+    return 0;
+}
+
+int Plan::execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
+                  float sInt, void* stream) {
+    if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull) return -8;
+    if (!validShape(n, (uint32_t)batch, kExecR2C)) return -8;
+    int e = 0, cta = 0;
+    resolve(backend::kR2C, n, &e, &cta);
+    if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
+    const bool weighted = !(sEdge == 1.0f && sInt == 1.0f);
+    if (backend::launchR2C(dIn, dOut, n, batch, impl_->twC2C[{n / 2, e}], impl_->twReal[n], e, cta,
+                           weighted, sEdge, sInt, stream ? stream : stream_))
+        return -5;
+    return 0;
+}
+
+int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
+                  float sInt, float outScale, void* stream) {
+    if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull) return -8;
+    if (!validShape(n, (uint32_t)batch, kExecC2R)) return -8;
+    int e = 0, cta = 0;
+    resolve(backend::kC2R, n, &e, &cta);
+    if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
+    if (backend::launchC2R(dIn, dOut, n, batch, impl_->twC2C[{n / 2, e}], impl_->twReal[n], e, cta,
+                           sEdge, sInt, outScale, stream ? stream : stream_))
+        return -5;
+    return 0;
+}
+
+// Shared body of the synchronous host-pointer entry points: upload, enqueue, sync, download.
+// enqueue() returns an exec* status: -2 prepare and -3 alloc pass through, others map to -5.
+template <class Enqueue>
+static int hostRoundTrip(void** dIn, size_t* inCap, void** dOut, size_t* outCap, void* stream,
+                         const float* in, size_t inBytes, float* out, size_t outBytes,
+                         Enqueue&& enqueue) {
+    if (ensureBuf(dIn, inCap, inBytes)) return -3;
+    if (ensureBuf(dOut, outCap, outBytes)) return -3;
+    if (backend::copyH2D(*dIn, in, inBytes, stream)) return -4;
+    const int lrc = enqueue(*dIn, *dOut);
+    if (lrc == -2 || lrc == -3) return lrc;
+    if (lrc) return -5;
+    if (backend::streamSync(stream)) return -6;
+    if (backend::copyD2H(out, *dOut, outBytes, stream)) return -7;
+    if (backend::streamSync(stream)) return -7;
+    return 0;
+}
+
+#define BFLY_ROUNDTRIP(inPtr, inBytes, outPtr, outBytes, body)                                   \
+    hostRoundTrip(&impl_->devIn, &impl_->devInCap, &impl_->devOut, &impl_->devOutCap, stream_,  \
+                  inPtr, inBytes, outPtr, outBytes, body)
+
+int Plan::run(const float* in, float* out, uint32_t n, uint32_t batch) {
+    if (!in || !out || !validShape(n, batch, kRunC2C)) return -8;
+    if (prepare(n, batch)) return -2;
+    const size_t bytes = (size_t)n * batch * 8;
+    return BFLY_ROUNDTRIP(in, bytes, out, bytes, [&](void* di, void* dout) {
+        return execC2C(di, dout, n, batch, -1, 1.0f, stream_);
+    });
+}
+
+int Plan::runInverse(const float* in, float* out, uint32_t n, uint32_t batch, float scale) {
+    if (!in || !out || !validShape(n, batch, kRunC2C)) return -8;
+    if (prepare(n, batch)) return -2;
+    const size_t bytes = (size_t)n * batch * 8;
+    return BFLY_ROUNDTRIP(in, bytes, out, bytes, [&](void* di, void* dout) {
+        return execC2C(di, dout, n, batch, 1, scale, stream_);
+    });
+}
+
+int Plan::runLong(const float* in, float* out, uint32_t n, uint32_t batch, int direction) {
+    if (!in || !out || (direction != -1 && direction != 1) || !validShape(n, batch, kRunLong)) return -8;
+    if (prepare(n, batch)) return -2;
+    const size_t bytes = (size_t)n * batch * 8;
+    return BFLY_ROUNDTRIP(in, bytes, out, bytes, [&](void* di, void* dout) {
+        return execC2C(di, dout, n, batch, direction, 1.0f, stream_);
+    });
+}
+
+int Plan::runR2C(const float* in, float* out, uint32_t n, uint32_t batch) {
+    if (!in || !out || !validShape(n, batch, kRunR2C)) return -8;
+    int e = 0, cta = 0;
+    resolve(backend::kR2C, n, &e, &cta);
+    if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
+    return BFLY_ROUNDTRIP(in, (size_t)n * batch * 4, out, (size_t)(n + 2) * batch * 4,
+                          [&](void* di, void* dout) {
+                             return execR2C(di, dout, n, batch, 1.0f, 1.0f, stream_);
+                         });
+}
+
+int Plan::runC2R(const float* in, float* out, uint32_t n, uint32_t batch) {
+    if (!in || !out || !validShape(n, batch, kRunC2R)) return -8;
+    int e = 0, cta = 0;
+    resolve(backend::kC2R, n, &e, &cta);
+    if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
+    return BFLY_ROUNDTRIP(in, (size_t)(n + 2) * batch * 4, out, (size_t)n * batch * 4,
+                          [&](void* di, void* dout) {
+                             return execC2R(di, dout, n, batch, 1.0f, 1.0f, 1.0f / (float)n, stream_);
+                         });
+}
+
+int Plan::measure(uint32_t n, uint32_t batch, Metric* m) {
+    if (!m) return -1;
+    if (!validShape(n, batch, kMeasure)) return -8;
+    const size_t nf = (size_t)n * 2 * batch;
+    std::vector<float> in(nf), out(nf);
+    for (size_t i = 0; i < nf; ++i) in[i] = patternAt(i);
+    if (prepare(n, batch)) return -2;
+    const int first = BFLY_ROUNDTRIP(in.data(), nf * 4, out.data(), nf * 4, [&](void* di, void* dout) {
+        return execC2C(di, dout, n, batch, -1, 1.0f, stream_);
+    });
+    if (first) return -2;
+    if (!impl_->timer && backend::timerCreate(&impl_->timer)) return -3;
+    // Device time per launch, best of 10 (CUDA events on the plan stream).
+    auto once = [&](float* ms) -> int {
+        if (backend::timerStart(impl_->timer, stream_)) return -3;
+        if (execC2C(impl_->devIn, impl_->devOut, n, batch, -1, 1.0f, stream_)) return -4;
+        if (backend::timerStop(impl_->timer, stream_, ms)) return -3;
+        return 0;
+    };
+    float ms = 0.f;
+    if (int r = once(&ms)) return r;   // warm-up
+    double best = 0.0;
+    for (int r = 0; r < 10; ++r) {
+        if (int e = once(&ms)) return e == -4 ? -5 : e;
+        if (r == 0 || ms * 1000.0 < best) best = ms * 1000.0;
+    }
+    m->measuredUs = best;
+    if (backend::copyD2H(out.data(), impl_->devOut, nf * 4, stream_) || backend::streamSync(stream_)) return -6;
+    m->etaUs = cand_.q.etaUs;
+    uint32_t idx[8];
+    const uint32_t cnt = sampleBatches(batch, 8, idx, 8);
+    std::vector<float> ref(2 * (size_t)n);
+    double maxRel = 0.0;
+    for (uint32_t i = 0; i < cnt; ++i) {
+        const size_t off = (size_t)idx[i] * 2 * n;
+        refFftF32(in.data() + off, ref.data(), n);
+        maxRel = std::max(maxRel, maxRelScaled(out.data() + off, ref.data(), 2 * (size_t)n));
+    }
+    m->maxRelErr = maxRel;
+    if (!std::isfinite(maxRel) || maxRel > 1e-4) {
+        m->measuredOk = false;
+        cand_.q = *m;
+        cand_.state = State::Unverified;
+        cand_.reason = "correctness check failed (maxRel > 1e-4)";
+        return -7;
+    }
+    m->measuredOk = true;
+    cand_.q = *m;
+    cand_.reason.clear();
+    cand_.state = State::Measured;
+    return 0;
+}
+
+// ================================================================== Context
+struct Context::Impl {
+    void* stream = nullptr;
+    bool initialized = false;
+};
+
+Context::Context() : impl_(new Impl) {}
+
+Context::~Context() {
+    if (impl_->stream) backend::streamDestroy(impl_->stream);
+}
+
+void* Context::stream() const { return impl_->stream; }
+
+int Context::init(const std::string& profilePath, const std::string& spacePath,
+                  const std::string& kernelPath) {
+    return init(profilePath, spacePath, kernelPath, -1);
+}
+
+int Context::init(const std::string& profilePath, const std::string& spacePath,
+                  const std::string& kernelPath, int device) {
+    if (impl_->initialized) return -9;
+    Hardware hardware;
+    DesignSpace space;
+    try {
+        hardware = Hardware::load(profilePath);
+        space = DesignSpace::load(spacePath);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "Context::init configuration error: %s\n", e.what());
+        return -4;
+    }
+    hw_ = std::move(hardware);
+    sp_ = std::move(space);
+    kernelPath_ = kernelPath;
+    if (device >= 0) hw_.deviceIndex = device;
+    int count = 0;
+    if (backend::deviceCount(&count) || count <= 0) return -1;
+    if (hw_.deviceIndex >= count || backend::setDevice(hw_.deviceIndex)) return -2;
+    if (backend::streamCreate(&impl_->stream)) return -3;
+    impl_->initialized = true;
+    return 0;
+}
+
+std::vector<Candidate> Context::enumerate(uint32_t n, uint32_t batch) const {
+    return bfly::enumerate(sp_, hw_, n, batch);
+}
+
+std::unique_ptr<Plan> Context::makePlan(const Candidate& c) {
+    if (!impl_->initialized || c.state == State::Infeasible || !lowerable(c, hw_)) return nullptr;
+    if (!kernelPath_.empty() && kernelPath_ != "builtin") {
+        std::ifstream f(kernelPath_, std::ios::binary);
+        if (!f) return nullptr;   // the named kernel library does not exist
+    }
+    auto p = std::unique_ptr<Plan>(new Plan(c));
+    p->impl_.reset(new Plan::Impl());
+    p->impl_->hw = hw_;
+    p->impl_->device = hw_.deviceIndex;
+    p->stream_ = impl_->stream;
+    p->tf_.push_back({Transform::GenTwiddles, "FP64 twiddle tables built on the device, rounded to fp32"});
+    p->tf_.push_back({Transform::LaunchKernel, "hand-written sm_100a kernels on the context stream"});
+    return p;
+}
+
+// ------------------------------------------------------------------ tuning cache
+namespace {
+struct CacheEntry {
+    std::string gpu, kind, id;
+    long long n = 0, batch = 0;
+    double us = 0.0;
+};
+
+std::vector<CacheEntry> readCache(const std::string& path) {
+    std::vector<CacheEntry> out;
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return out;
+    try {
+        const std::string text((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+        const json::Node root = json::parse(text);
+        if (root.get("schema_version").asInt() != 1) return out;
+        for (const auto& e : root.get("entries").items) {
+            CacheEntry c;
+            c.gpu = e.get("gpu").asString();
+            c.kind = e.get("kind").asString();
+            c.id = e.get("id").asString();
+            c.n = e.get("n").asInt();
+            c.batch = e.get("batch").asInt();
+            c.us = e.get("us").asDouble();
+            out.push_back(c);
+        }
+    } catch (const std::exception&) {
+        out.clear();   // an unreadable cache is ignored and rewritten
+    }
+    return out;
+}
+
+std::string escapeJson(const std::string& s) {
+    std::string o;
+    for (char ch : s) {
+        if (ch == '"' || ch == '\\') o += '\\';
+        if ((unsigned char)ch >= 0x20) o += ch;
+    }
+    return o;
+}
+
+void writeCache(const std::string& path, const std::vector<CacheEntry>& es) {
+    std::ostringstream os;
+    os << "{\n  \"schema_version\": 1,\n  \"entries\": [";
+    for (size_t i = 0; i < es.size(); ++i) {
+        const auto& e = es[i];
+        char us[64];
+        std::snprintf(us, sizeof(us), "%.3f", e.us);
+        os << (i ? ",\n" : "\n") << "    {\"gpu\": \"" << escapeJson(e.gpu) << "\", \"kind\": \""
+           << escapeJson(e.kind) << "\", \"n\": " << e.n << ", \"batch\": " << e.batch
+           << ", \"id\": \"" << escapeJson(e.id) << "\", \"us\": " << us << "}";
+    }
+    os << "\n  ]\n}\n";
+    const std::string tmp = path + ".tmp";
+    {
+        std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
+        if (!f) return;
+        f << os.str();
+        if (!f) return;
+    }
+    std::rename(tmp.c_str(), path.c_str());
+}
+}  // namespace
+
+std::unique_ptr<Plan> Context::select(uint32_t n, uint32_t batch, int topK, std::string* log) {
+    auto all = enumerate(n, batch);
+    auto order = rank(all);
+    const int k = std::max(1, topK);
+    char line[512];
+    if (log) {
+        log->clear();
+        int infeasible = 0;
+        for (const auto& c : all) infeasible += c.state == State::Infeasible;
+        std::snprintf(line, sizeof(line), "enumerated=%zu infeasible=%d feasible=%zu (n=%u batch=%u)\n",
+                      all.size(), infeasible, order.size(), n, batch);
+        *log += line;
+        std::vector<std::pair<int, std::string>> reasons;
+        for (const auto& c : all) {
+            if (c.state != State::Infeasible) continue;
+            bool hit = false;
+            for (auto& r : reasons)
+                if (r.second == c.reason) { ++r.first; hit = true; break; }
+            if (!hit) reasons.push_back({1, c.reason});
+        }
+        std::stable_sort(reasons.begin(), reasons.end(), [](auto& x, auto& y) { return x.first > y.first; });
+        for (size_t i = 0; i < reasons.size() && i < 5; ++i) {
+            std::snprintf(line, sizeof(line), "  infeasible x%-4d %s\n", reasons[i].first, reasons[i].second.c_str());
+            *log += line;
+        }
+        std::snprintf(line, sizeof(line), "  eta rank (top %d):\n", k);
+        *log += line;
+        for (size_t i = 0; i < order.size() && i < (size_t)k; ++i) {
+            std::snprintf(line, sizeof(line), "    %2zu. %-44s eta=%8.1f us  [%s]\n", i + 1,
+                          order[i]->id.c_str(), order[i]->q.etaUs, toString(order[i]->state));
+            *log += line;
+        }
+    }
+    if (order.empty()) return nullptr;
+
+    // Persisted choice for this (gpu, n, batch)?
+    std::vector<CacheEntry> cache;
+    if (!tuningCache_.empty()) {
+        cache = readCache(tuningCache_);
+        for (const auto& e : cache) {
+            if (e.gpu != hw_.gpu || e.kind != "c2c" || e.n != n || e.batch != batch) continue;
+            for (const Candidate* c : order) {
+                if (c->id != e.id) continue;
+                auto p = makePlan(*c);
+                if (p) {
+                    if (log) {
+                        std::snprintf(line, sizeof(line), "  selected: %s  (tuning cache, %.1f us)\n", c->id.c_str(), e.us);
+                        *log += line;
+                    }
+                    return p;
+                }
+            }
+        }
+    }
+
+    if (log) *log += "  measured selection:\n";
+    std::unique_ptr<Plan> best;
+    double bestUs = 0.0;
+    int measured = 0;
+    size_t examined = 0;
+    for (size_t i = 0; i < order.size() && measured < k; ++i) {
+        ++examined;
+        const Candidate& c = *order[i];
+        auto p = makePlan(c);
+        if (!p) {
+            if (log) {
+                std::snprintf(line, sizeof(line), "    fail   %-44s eta=%8.1f us  makePlan failed\n", c.id.c_str(), c.q.etaUs);
+                *log += line;
+            }
+            continue;
+        }
+        Metric m;
+        const int rc = p->measure(n, batch, &m);
+        if (rc) {
+            if (log) {
+                std::snprintf(line, sizeof(line), "    reject %-44s eta=%8.1f us  rc=%d maxRel=%.2e  [%s]\n",
+                              c.id.c_str(), c.q.etaUs, rc, m.maxRelErr, toString(p->candidate().state));
+                *log += line;
+            }
+            continue;
+        }
+        ++measured;
+        if (log) {
+            std::snprintf(line, sizeof(line), "    accept %-44s eta=%8.1f us  measured=%8.1f us  maxRel=%.1e  [%s]\n",
+                          p->candidate().id.c_str(), m.etaUs, m.measuredUs, m.maxRelErr,
+                          toString(p->candidate().state));
+            *log += line;
+        }
+        if (!best || m.measuredUs < bestUs) {
+            bestUs = m.measuredUs;
+            best = std::move(p);
+        }
+    }
+    if (log) {
+        if (best)
+            std::snprintf(line, sizeof(line), "  selected: %s  (%.1f us, %d accepted after %zu examined, quota %d)\n",
+                          best->candidate().id.c_str(), bestUs, measured, examined, k);
+        else
+            std::snprintf(line, sizeof(line), "  selected: none (%d accepted after %zu examined, quota %d)\n",
+                          measured, examined, k);
+        *log += line;
+    }
+    if (best && !tuningCache_.empty()) {
+        cache.erase(std::remove_if(cache.begin(), cache.end(), [&](const CacheEntry& e) {
+                        return e.gpu == hw_.gpu && e.kind == "c2c" && e.n == n && e.batch == batch;
+                    }), cache.end());
+        cache.push_back({hw_.gpu, "c2c", best->candidate().id, (long long)n, (long long)batch, bestUs});
+        writeCache(tuningCache_, cache);
+    }
+    return best;
+}
+
+}  // namespace bfly

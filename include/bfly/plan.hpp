@@ -1,0 +1,226 @@
+// bfly::Context / bfly::Plan for NVIDIA B200 (sm_100a): the C++ host API of the batched
+// power-of-two fp32 FFT library.  It keeps the surface of the reference's plan API
+// (include/butterfly/plan.hpp:26-91 of TruNcat3/ascend-fft) so code written against it ports
+// by changing the configuration files:
+//   Context::init(profile, space, kernel)  -> 0 | -1 runtime | -2 device | -3 stream |
+//                                             -4 configuration | -9 already initialised
+//   Context::enumerate / select / makePlan
+//   Plan::prepare / run / runR2C / runC2R / measure with the same status codes:
+//     0 ok, -1 kernel not available, -2 prepare, -3 alloc, -4 H2D, -5 launch, -6 sync,
+//     -7 D2H (measure: acceptance failure), -8 shape / guard (checked before any allocation)
+// Additions for the B200 build: inverse C2C, long C2C (four-step, 8192..65536), and the
+// asynchronous device-pointer entry points exec* that never cross the host/device boundary.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace bfly {
+
+// ---------------------------------------------------------------- H: hardware profile
+struct Hardware {
+    std::string gpu;            // e.g. "NVIDIA B200"
+    std::string arch;           // "sm_100a"
+    int deviceIndex = 0;
+    int smCount = 0;
+    int smemPerCta = 0;         // opt-in maximum dynamic shared memory per CTA (bytes)
+    int smemPerSm = 0;
+    int regsPerSm = 0;
+    int maxThreadsPerSm = 0;
+    long long l2Bytes = 0;
+    double hbmGbs = 0;          // measured copy bandwidth, the roofline denominator
+
+    // Throws std::exception for unreadable, malformed or invalid configuration.
+    static Hardware load(const std::string& profilePath);
+};
+
+// ---------------------------------------------------------------- A: mapping
+struct Mapping {
+    int ctaThreads = 256;                  // threads per CTA
+    std::string localExchange = "shared";  // shared | shuffle (not lowered)
+    int level = 0;                         // 0 = one GPU (batch sharding lives above the plan)
+    bool validate(const Hardware& hw, std::string* why) const;
+};
+
+// ---------------------------------------------------------------- P: stage plan
+struct StagePlan {
+    int radix = 16;                        // complex values per thread = register radix
+    bool coefficientResidency = true;      // twiddle tables read through L1
+    int fusionLevel = 1;                   // passes per kernel launch granularity (1 = all)
+    // Dynamic shared memory of the single-pass kernel for complex length n.
+    size_t smemBytes(uint32_t n, int ctaThreads) const;
+};
+
+// ---------------------------------------------------------------- L: layout
+struct Layout {
+    enum Pack : uint8_t { Interleaved = 0, Planar = 1 };
+    Pack in = Interleaved;
+    Pack out = Interleaved;
+    bool contiguous = true;
+};
+
+// ---------------------------------------------------------------- F: fusion / schedule
+struct Fusion {
+    std::string precision = "fp32";        // fp32 | split_bf16
+    std::string schedule = "stockham";     // stockham (one pass) | four_step (two passes)
+};
+
+// ---------------------------------------------------------------- Q: quality / metric
+struct Metric {
+    double etaUs = 0.0;       // model estimate (µs)
+    double measuredUs = 0.0;  // best device time over the timed launches (µs)
+    double maxRelErr = 0.0;   // maxRelScaled against the FP64 acceptance reference
+    bool measuredOk = false;
+};
+
+enum class State : uint8_t { Infeasible = 0, Unverified = 1, Feasible = 2, Measured = 3 };
+const char* toString(State s);
+
+struct Candidate {
+    std::string id;
+    Mapping a;
+    StagePlan p;
+    Layout l;
+    Fusion f;
+    Metric q;
+    State state = State::Unverified;
+    std::string reason;       // why Infeasible
+};
+
+struct DesignSpace {
+    std::vector<int> ctaThreads;
+    std::vector<int> radices;
+    std::vector<int> fusionStages;
+    std::vector<int> coeffResidency;
+    std::vector<std::string> localExchanges;
+    std::vector<std::string> layoutsIn;
+    std::vector<std::string> layoutsOut;
+    std::vector<std::string> precisions;
+    std::vector<std::string> schedules;
+    std::string raw;
+
+    // Strict loading; missing or malformed files or axes throw std::exception.
+    static DesignSpace load(const std::string& path);
+    void applyDefaults();
+};
+
+// Enumerate the Cartesian product of the space axes for a C2C transform of length n.
+std::vector<Candidate> enumerate(const DesignSpace& sp, const Hardware& hw, uint32_t n,
+                                 uint32_t batch);
+// Non-infeasible candidates, Measured first, then ascending estimate.
+std::vector<const Candidate*> rank(const std::vector<Candidate>& cs);
+Metric estimate(const Hardware& hw, const Candidate& c, uint32_t n, uint32_t batch);
+
+class Transform {
+public:
+    enum Kind : uint8_t { GenTwiddles, GenBitReverse, LaunchKernel, Measure } kind;
+    std::string label;
+};
+
+class Context;
+
+class Plan {
+public:
+    ~Plan();
+    const Candidate& candidate() const { return cand_; }
+    const std::vector<Transform>& transforms() const { return tf_; }
+
+    // Build (idempotently) the FP64-generated twiddle tables for a C2C of length n.
+    int prepare(uint32_t n, uint32_t batch = 0xFFFFFFFFu);
+    // Synchronous host-pointer entry points (reference semantics and envelopes):
+    //   run     C2C forward, n in [64, 4096], in/out [batch][2n]
+    //   runR2C  in [batch][n] real -> out [batch][n+2], n in [128, 8192]
+    //   runC2R  in [batch][n+2] -> out [batch][n] real incl. 1/n, n in [64, 4096]
+    // batch > 0, non-null pointers, batch*2n <= 2^32-1; otherwise -8 before any allocation.
+    int run(const float* in, float* out, uint32_t n, uint32_t batch);
+    int runR2C(const float* in, float* out, uint32_t n, uint32_t batch);
+    int runC2R(const float* in, float* out, uint32_t n, uint32_t batch);
+    int measure(uint32_t n, uint32_t batch, Metric* out);
+
+    // B200 additions (synchronous, host pointers)
+    int runInverse(const float* in, float* out, uint32_t n, uint32_t batch, float scale);
+    int runLong(const float* in, float* out, uint32_t n, uint32_t batch, int direction);
+
+    // Asynchronous device-pointer entry points: enqueue on `stream` (nullptr = the context
+    // stream) and return; no host synchronisation, no host<->device copies.
+    //   direction -1 forward, +1 inverse; scale multiplies the output.
+    //   n in [32, 16384] single pass, [8192, 65536] four-step (workspace grown on demand).
+    int execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
+                float scale, void* stream);
+    // R2C [batch][n] -> [batch][n/2+1] complex, bins scaled by (sEdge at 0 and n/2, sInt
+    // elsewhere); sEdge = sInt = 1 is the plain transform.
+    int execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
+                float sInt, void* stream);
+    // C2R [batch][n/2+1] -> [batch][n]; input bins scaled by sEdge/sInt, output by outScale
+    // (1/n = numpy.fft.irfft).
+    int execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
+                float sInt, float outScale, void* stream);
+
+    void* stream() const { return stream_; }
+
+private:
+    friend class Context;
+    explicit Plan(Candidate c);
+    struct Impl;
+    bool validShape(uint32_t n, uint32_t batch, int kind) const;
+    int prepareC2C(uint32_t n, int e);
+    int prepareReal(uint32_t n);
+    int prepareLong(uint32_t n);
+    int resolve(int kind, uint32_t n, int* e, int* cta) const;
+    Candidate cand_;
+    std::vector<Transform> tf_;
+    std::unique_ptr<Impl> impl_;
+    void* stream_ = nullptr;   // owned by the Context
+};
+
+class Context {
+public:
+    Context();
+    ~Context();
+
+    // Configuration errors return -4; repeated initialisation returns -9.
+    // kernelPath: "builtin" (or empty) selects the kernels compiled into this library;
+    // any other value must name an existing file (the library itself), else makePlan fails.
+    int init(const std::string& profilePath, const std::string& spacePath,
+             const std::string& kernelPath);
+    // Same, with the profile's device_index replaced by `device` (one process per GPU).
+    int init(const std::string& profilePath, const std::string& spacePath,
+             const std::string& kernelPath, int device);
+    const Hardware& hardware() const { return hw_; }
+    const DesignSpace& space() const { return sp_; }
+    const std::string& kernelPath() const { return kernelPath_; }
+
+    std::vector<Candidate> enumerate(uint32_t n, uint32_t batch) const;
+    // Autotuner: rank by estimate, build and measure candidates until topK pass the FP64
+    // acceptance check, keep the fastest.  With a tuning cache set, a cached choice for
+    // (gpu, n, batch) is returned without measuring and new choices are persisted.
+    std::unique_ptr<Plan> select(uint32_t n, uint32_t batch, int topK = 3,
+                                 std::string* log = nullptr);
+    std::unique_ptr<Plan> makePlan(const Candidate& c);
+    // Persist autotuned choices in a JSON file; "" disables.
+    void setTuningCache(const std::string& path) { tuningCache_ = path; }
+    void* stream() const;
+
+private:
+    Hardware hw_;
+    DesignSpace sp_;
+    std::string kernelPath_;
+    std::string tuningCache_;
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
+
+// ---------------------------------------------------------------- acceptance helpers
+// FP64 reference transforms used by Plan::measure's acceptance check (outputs rounded to fp32),
+// with the semantics of the reference's include/butterfly/reference.hpp.
+void refFftF32(const float* in, float* out, uint32_t n);
+void refR2CF32(const float* in, float* out, uint32_t n);
+void refC2RF32(const float* in, float* out, uint32_t n);
+// max|got-ref| / max(1, max|ref|) over float components; non-finite -> infinity.
+double maxRelScaled(const float* got, const float* ref, size_t len);
+float patternAt(size_t i);
+uint32_t sampleBatches(uint32_t batch, uint32_t want, uint32_t* out, uint32_t maxOut);
+
+}  // namespace bfly

@@ -1,0 +1,135 @@
+/* C ABI of the B200 batched FFT library (libbfly_b200.so).
+ *
+ * Plain pointers, sizes and int status codes; no C++ or torch types.  Each entry point
+ * replaces one method of the reference's C++ plan API (TruNcat3/ascend-fft,
+ * include/butterfly/plan.hpp; implementation src/framework/butterfly.cpp), cited beside it.
+ *
+ * Status codes (reference docs/reference/api.md:34-50):
+ *   context init: 0 ok, -1 runtime, -2 device, -3 stream, -4 configuration, -9 re-init
+ *   plan calls:   0 ok, -1 kernel unavailable, -2 prepare, -3 alloc, -4 H2D, -5 launch,
+ *                 -6 sync, -7 D2H (measure: acceptance failed), -8 shape/guard
+ *   C ABI only:   -10 null handle / argument, -11 buffer too small
+ *
+ * Layouts: complex data is interleaved fp32 [re, im]; C2C rows are [batch][2n] floats,
+ * R2C output / C2R input rows are [batch][n+2] floats (n/2+1 complex bins).
+ * Threading: one thread at a time per plan; a context owns one CUDA stream.
+ */
+#ifndef BFLY_B200_H
+#define BFLY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bfly_context bfly_context;
+typedef struct bfly_plan bfly_plan;
+
+typedef struct bfly_metric {
+    double eta_us;
+    double measured_us;
+    double max_rel_err;
+    int measured_ok;
+} bfly_metric;
+
+/* Library version string. */
+const char* bfly_version(void);
+
+/* Context lifetime; replaces bfly::Context::Context / ~Context (plan.hpp:62-63). */
+int bfly_context_create(bfly_context** out);
+void bfly_context_destroy(bfly_context* ctx);
+
+/* Replaces Context::init(profilePath, spacePath, kernelPath) (plan.hpp:68,
+ * butterfly.cpp:938-958).  kernel_path "builtin" selects the kernels compiled into this
+ * library. */
+int bfly_context_init(bfly_context* ctx, const char* profile_path, const char* space_path,
+                      const char* kernel_path);
+/* Same, overriding the profile's device_index (one process per GPU). */
+int bfly_context_init_device(bfly_context* ctx, const char* profile_path,
+                             const char* space_path, const char* kernel_path, int device);
+
+/* Replaces Context::enumerate (plan.hpp:75): writes "id\tstate\treason\n" lines into buf
+ * (NUL-terminated); *count receives the number of candidates, *needed the bytes required. */
+int bfly_context_enumerate(bfly_context* ctx, uint32_t n, uint32_t batch, char* buf,
+                           size_t cap, int* count, size_t* needed);
+
+/* Replaces Context::select(n, batch, topK, log) (plan.hpp:78, butterfly.cpp:999-1102):
+ * the measuring autotuner.  log may be NULL; otherwise up to log_cap bytes are written. */
+int bfly_context_select(bfly_context* ctx, uint32_t n, uint32_t batch, int top_k,
+                        bfly_plan** out, char* log, size_t log_cap);
+
+/* Replaces Context::makePlan(candidate) (plan.hpp:82): the candidate is named by the id
+ * printed by enumerate. */
+int bfly_context_make_plan(bfly_context* ctx, uint32_t n, uint32_t batch,
+                           const char* candidate_id, bfly_plan** out);
+
+/* Persist autotuner choices in a JSON file (new; the reference re-measures every select). */
+int bfly_context_set_tuning_cache(bfly_context* ctx, const char* path);
+
+/* The context's CUDA stream (cudaStream_t as void*). */
+void* bfly_context_stream(bfly_context* ctx);
+
+/* Replaces Plan::~Plan (plan.hpp:28). */
+void bfly_plan_destroy(bfly_plan* plan);
+
+/* Candidate id of the plan into buf. */
+int bfly_plan_candidate_id(bfly_plan* plan, char* buf, size_t cap);
+
+/* Replaces Plan::prepare(n, batch) (plan.hpp:34, butterfly.cpp:587-658). */
+int bfly_plan_prepare(bfly_plan* plan, uint32_t n, uint32_t batch);
+
+/* Replaces Plan::run (plan.hpp:37, butterfly.cpp:723-749): synchronous C2C forward of host
+ * buffers [batch][2n], n in [64, 4096]. */
+int bfly_plan_run_c2c(bfly_plan* plan, const float* in, float* out, uint32_t n, uint32_t batch);
+
+/* Replaces Plan::runR2C (plan.hpp:40, butterfly.cpp:753-806): [batch][n] -> [batch][n+2],
+ * n in [128, 8192]. */
+int bfly_plan_run_r2c(bfly_plan* plan, const float* in, float* out, uint32_t n, uint32_t batch);
+
+/* Replaces Plan::runC2R (plan.hpp:43, butterfly.cpp:810-850): [batch][n+2] -> [batch][n]
+ * including 1/n, n in [64, 4096]. */
+int bfly_plan_run_c2r(bfly_plan* plan, const float* in, float* out, uint32_t n, uint32_t batch);
+
+/* Replaces Plan::measure (plan.hpp:45, butterfly.cpp:852-924). */
+int bfly_plan_measure(bfly_plan* plan, uint32_t n, uint32_t batch, bfly_metric* out);
+
+/* New: synchronous inverse C2C (unnormalised inverse times scale), n in [64, 4096].
+ * The reference has no public inverse; it is implied by its C2R sign flip
+ * (src/ascendc/fft_real.cpp:6-7). */
+int bfly_plan_run_c2c_inverse(bfly_plan* plan, const float* in, float* out, uint32_t n,
+                              uint32_t batch, float scale);
+
+/* New: synchronous long C2C via four-step, n in [8192, 65536], direction -1 / +1.
+ * Replaces the harness-only four-step chain (src/host/fft_check.cpp:289-362, 843-970). */
+int bfly_plan_run_c2c_long(bfly_plan* plan, const float* in, float* out, uint32_t n,
+                           uint32_t batch, int direction);
+
+/* New asynchronous device-pointer entry points.  Enqueue on `stream` (cudaStream_t; NULL =
+ * the context stream) and return without synchronising.  The first call for a length builds
+ * its twiddle tables (and the four-step workspace) and synchronises the context stream once;
+ * make it before any stream capture. */
+/* C2C, n in [32, 65536]; direction -1 forward / +1 inverse; output multiplied by scale. */
+int bfly_plan_exec_c2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
+                             uint64_t batch, int direction, float scale, void* stream);
+/* R2C [batch][n] -> [batch][n/2+1] complex, n in [64, 8192]; bins 0 and n/2 scaled by
+ * s_edge, the others by s_int (1, 1 for the plain transform). */
+int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
+                             uint64_t batch, float s_edge, float s_int, void* stream);
+/* C2R [batch][n/2+1] -> [batch][n], n in [64, 8192]; input bins scaled by s_edge / s_int,
+ * output by out_scale (1/n is numpy.fft.irfft). */
+int bfly_plan_exec_c2r_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
+                             uint64_t batch, float s_edge, float s_int, float out_scale,
+                             void* stream);
+
+/* Acceptance helpers with the reference's semantics (include/butterfly/reference.hpp:14-60). */
+double bfly_max_rel_scaled(const float* got, const float* ref, size_t len);
+float bfly_pattern_at(size_t i);
+uint32_t bfly_sample_batches(uint32_t batch, uint32_t want, uint32_t* out, uint32_t max_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BFLY_B200_H */
