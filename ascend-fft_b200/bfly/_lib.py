@@ -45,10 +45,21 @@ SIGNATURES = {
                                            C.c_float, C.c_float, C.c_void_p]),
     "bfly_plan_exec_c2r_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
                                            C.c_float, C.c_float, C.c_float, C.c_void_p]),
+    "bfly_ragged_create": (C.c_int, [c_plan, C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "bfly_ragged_exec_async": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfly_ragged_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),
+    "bfly_ragged_destroy": (None, [C.c_void_p]),
     "bfly_max_rel_scaled": (C.c_double, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "bfly_pattern_at": (C.c_float, [C.c_size_t]),
     "bfly_sample_batches": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]),
 }
+
+
+class RaggedRequest(C.Structure):
+    """bfly_ragged_request of include/bfly_b200.h."""
+    _fields_ = [("d_in", C.c_void_p), ("d_out", C.c_void_p), ("n", C.c_uint32),
+                ("direction", C.c_int32), ("batch", C.c_uint64), ("scale", C.c_float),
+                ("reserved", C.c_uint32)]
 
 
 class Metric(C.Structure):

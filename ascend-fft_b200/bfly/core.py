@@ -159,9 +159,51 @@ class Plan:
         return self._lib.bfly_plan_exec_c2r_async(self._h, d_in, d_out, n, batch, s_edge, s_int,
                                                   out_scale, stream or None)
 
+    def make_ragged(self, requests):
+        """requests: iterable of (d_in, d_out, n, batch, direction, scale) with device
+        pointers; returns a Ragged whose exec(stream) is one persistent kernel launch."""
+        reqs = list(requests)
+        arr = (_lib.RaggedRequest * len(reqs))()
+        for i, (din, dout, n, b, d, sc) in enumerate(reqs):
+            arr[i] = _lib.RaggedRequest(din, dout, n, d, b, sc, 0)
+        h = C.c_void_p()
+        rc = self._lib.bfly_ragged_create(self._h, arr, len(reqs), C.byref(h))
+        if rc:
+            raise BflyError("bfly_ragged_create", rc)
+        return Ragged(self, h)
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.bfly_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Ragged:
+    """One persistent launch over many C2C requests (bfly_ragged_* of the C ABI)."""
+
+    def __init__(self, plan: Plan, handle: C.c_void_p):
+        self._plan = plan   # the ragged work list uses the plan's twiddle tables
+        self._lib = plan._lib
+        self._h = handle
+
+    def exec(self, stream: int = 0) -> int:
+        return self._lib.bfly_ragged_exec_async(self._h, stream or None)
+
+    def info(self):
+        tiles = C.c_uint64()
+        grid = C.c_int()
+        self._lib.bfly_ragged_info(self._h, C.byref(tiles), C.byref(grid))
+        return {"tiles": tiles.value, "grid": grid.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bfly_ragged_destroy(self._h)
             self._h = None
 
     def __del__(self):

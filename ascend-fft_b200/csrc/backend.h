@@ -64,5 +64,10 @@ int launchLongA(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
 int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t batch,
                 bool inverse, float scale, const void* tw2, void* stream);
 
+// Ragged persistent launch over a device array of RaggedEntry (ragged.h).
+int raggedSmemBytes();
+int raggedGrid(int device, int* grid);   // resident CTAs on the whole device
+int launchRagged(const void* entries, int count, uint64_t totalTiles, int grid, void* stream);
+
 }  // namespace backend
 }  // namespace bfly

@@ -7,12 +7,16 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <vector>
 
 struct bfly_context {
     bfly::Context ctx;
 };
 struct bfly_plan {
     std::unique_ptr<bfly::Plan> plan;
+};
+struct bfly_ragged {
+    std::unique_ptr<bfly::Ragged> ragged;
 };
 
 namespace {
@@ -175,6 +179,35 @@ int bfly_plan_exec_c2r_async(bfly_plan* plan, const void* d_in, void* d_out, uin
     PLAN_OR_FAIL();
     return p.execC2R(d_in, d_out, n, batch, s_edge, s_int, out_scale, stream);
 }
+
+int bfly_ragged_create(bfly_plan* plan, const bfly_ragged_request* reqs, size_t count,
+                       bfly_ragged** out) {
+    if (!plan || !plan->plan || !out) return -10;
+    *out = nullptr;
+    if (!reqs || count == 0) return -8;
+    std::vector<bfly::RaggedRequest> rs(count);
+    for (size_t i = 0; i < count; ++i)
+        rs[i] = {reqs[i].d_in, reqs[i].d_out, reqs[i].n, reqs[i].batch, reqs[i].direction, reqs[i].scale};
+    int status = 0;
+    auto r = plan->plan->makeRagged(rs.data(), count, &status);
+    if (!r) return status ? status : -1;
+    *out = new bfly_ragged{std::move(r)};
+    return 0;
+}
+
+int bfly_ragged_exec_async(bfly_ragged* ragged, void* stream) {
+    if (!ragged || !ragged->ragged) return -10;
+    return ragged->ragged->exec(stream);
+}
+
+int bfly_ragged_info(bfly_ragged* ragged, uint64_t* tiles, int* grid) {
+    if (!ragged || !ragged->ragged) return -10;
+    if (tiles) *tiles = ragged->ragged->tiles();
+    if (grid) *grid = ragged->ragged->grid();
+    return 0;
+}
+
+void bfly_ragged_destroy(bfly_ragged* ragged) { delete ragged; }
 
 double bfly_max_rel_scaled(const float* got, const float* ref, size_t len) {
     return bfly::maxRelScaled(got, ref, len);

@@ -12,6 +12,7 @@
 
 #include "backend.h"
 #include "json_config.hpp"
+#include "ragged.h"
 
 #include <algorithm>
 #include <cmath>
@@ -492,7 +493,7 @@ int Plan::execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int d
     if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull || (direction != -1 && direction != 1))
         return -8;
     if (!validShape(n, (uint32_t)batch, kExecC2C)) return -8;
-    void* s = stream ? stream : stream_;
+    void* s = stream;   // NULL is the CUDA default stream
     const bool inv = direction > 0;
     int e = 0, cta = 0;
     resolve(backend::kC2C, n, &e, &cta);
@@ -523,7 +524,7 @@ int Plan::execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
     const bool weighted = !(sEdge == 1.0f && sInt == 1.0f);
     if (backend::launchR2C(dIn, dOut, n, batch, impl_->twC2C[{n / 2, e}], impl_->twReal[n], e, cta,
-                           weighted, sEdge, sInt, stream ? stream : stream_))
+                           weighted, sEdge, sInt, stream))
         return -5;
     return 0;
 }
@@ -536,7 +537,7 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
     resolve(backend::kC2R, n, &e, &cta);
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
     if (backend::launchC2R(dIn, dOut, n, batch, impl_->twC2C[{n / 2, e}], impl_->twReal[n], e, cta,
-                           sEdge, sInt, outScale, stream ? stream : stream_))
+                           sEdge, sInt, outScale, stream))
         return -5;
     return 0;
 }
@@ -663,6 +664,62 @@ int Plan::measure(uint32_t n, uint32_t batch, Metric* m) {
     cand_.reason.clear();
     cand_.state = State::Measured;
     return 0;
+}
+
+// ================================================================== ragged
+Ragged::~Ragged() {
+    if (entries_) backend::release(entries_);
+}
+
+int Ragged::exec(void* stream) const {
+    return backend::launchRagged(entries_, (int)count_, total_, grid_, stream) ? -5 : 0;
+}
+
+std::unique_ptr<Ragged> Plan::makeRagged(const RaggedRequest* reqs, size_t count, int* status) {
+    int dummy = 0;
+    int& st = status ? *status : dummy;
+    st = -8;
+    if (!impl_ || !reqs || count == 0 || count > (1u << 24)) return nullptr;
+    for (size_t i = 0; i < count; ++i) {
+        const RaggedRequest& r = reqs[i];
+        if (!r.in || !r.out || !pow2(r.n) || r.n < kRaggedMinN || r.n > kRaggedMaxN || r.batch == 0 ||
+            (r.direction != -1 && r.direction != 1))
+            return nullptr;
+    }
+    std::vector<RaggedEntry> es(count);
+    uint64_t tile = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const RaggedRequest& r = reqs[i];
+        if (prepareC2C(r.n, kRaggedE)) {
+            st = -2;
+            return nullptr;
+        }
+        int logn = 0;
+        while ((1u << logn) < r.n) ++logn;
+        const uint32_t rows = (uint32_t)kRaggedThreads / (r.n / (uint32_t)kRaggedE);
+        es[i] = RaggedEntry{r.in, r.out, impl_->twC2C[{r.n, kRaggedE}], r.batch, tile, (uint32_t)logn,
+                            r.direction, r.scale, rows, 0};
+        tile += (r.batch + rows - 1) / rows;
+    }
+    std::unique_ptr<Ragged> rg(new Ragged());
+    rg->count_ = count;
+    rg->total_ = tile;
+    if (backend::raggedGrid(impl_->device, &rg->grid_)) {
+        st = -1;
+        return nullptr;
+    }
+    if (backend::alloc(&rg->entries_, count * sizeof(RaggedEntry))) {
+        rg->entries_ = nullptr;
+        st = -3;
+        return nullptr;
+    }
+    if (backend::copyH2D(rg->entries_, es.data(), count * sizeof(RaggedEntry), stream_) ||
+        backend::streamSync(stream_)) {
+        st = -4;
+        return nullptr;
+    }
+    st = 0;
+    return rg;
 }
 
 // ================================================================== Context

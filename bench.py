@@ -1,0 +1,462 @@
+"""Benchmark of the batched FFT library on B200 (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): plain fp32 C2C forward over
+the 49-point grid N in {64..4096} x batch in {1..4096}, interleaved complex, Re/Im i.i.d.
+N(0,1) seeded per point (seed = 1000*log2 N + log2 batch + 1).  One step = one forward
+transform of every grid point (49 kernel launches, captured in a CUDA graph) on inputs resident
+in HBM.  The step touches 355 MB of input and 355 MB of output, more than the 126 MB L2, so
+no explicit flush is needed between steps.
+
+  value      algorithmic bytes (16 * N * batch summed over the grid) / device time per step
+  e2e        the same metric through the C ABI's synchronous host-pointer entry point
+             (bfly_plan_run_c2c) with pinned host buffers: H2D + kernel + D2H timed per step
+  roofline   the dominant launch (N=4096, batch=4096) timed alone with CUDA events on its
+             stream against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own CPU FFT (its FP64 oracle src/framework/reference.cpp,
+             compiled from its sources into oracle/_ref) on a bounded sample of the grid,
+             rows spread over the host's threads
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun every rank runs the grid on its own GPU (weak scaling; no data-path
+collective) and rank 0 prints the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for p in (str(ROOT / "ascend-fft_b200"), str(ROOT)):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "FFT GB/s & %HBM roofline: plain FP32 vs TC split-BF16, fwd+bwd, rel err<=2e-6"
+UNIT = "GB/s"
+GRID_N = [64, 128, 256, 512, 1024, 2048, 4096]
+GRID_B = [1, 4, 16, 64, 256, 1024, 4096]
+DOMINANT = (4096, 4096)
+WORKLOAD = ("c2c_fwd_grid49: plain fp32 C2C forward over N{64..4096} x batch{1..4096}, "
+            "interleaved complex64, N(0,1) seeded per point")
+
+
+def grid_seed(n, b):
+    return 1000 * (n.bit_length() - 1) + (b.bit_length() - 1) + 1
+
+
+def grid_bytes():
+    return sum(16 * n * b for n in GRID_N for b in GRID_B)
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dominant_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, or None."""
+    p = ROOT / "profiles" / "roofline_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) == 2 and parts[0] == "c2c_fwd_n4096_b4096":
+            return int(parts[1])
+    return None
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU reference
+def cpu_reference_sample(rows_cap: int, budget_s: float, threads: int):
+    """The reference's own CPU FFT (oracle/_ref) over the grid with at most rows_cap rows per
+    point; falls back to the C restatement when the reference library is absent.
+    Returns (GB/s, seconds, bytes, kind, sample description)."""
+    from oracle import clib
+    kind = "reference"
+    lib = clib.reference()
+    if lib is not None:
+        fn = lib.ref_fft_rows
+    else:
+        kind = "port"
+        rest = clib.restatement()
+
+        def fn(xp, yp, n, rows):
+            for r in range(rows):
+                rest.orc_ref_fft(xp + r * 8 * n, yp + r * 8 * n, n)
+    jobs = []
+    for n in GRID_N:
+        for b in GRID_B:
+            rows = min(b, rows_cap)
+            rng = np.random.default_rng(grid_seed(n, b))
+            x = rng.standard_normal((rows, 2 * n)).astype(np.float32)
+            jobs.append((n, x, np.empty_like(x)))
+    chunks = []
+    for n, x, y in jobs:
+        step = max(1, x.shape[0] // threads)
+        for r0 in range(0, x.shape[0], step):
+            r1 = min(x.shape[0], r0 + step)
+            chunks.append((n, x, y, r0, r1))
+    nbytes = sum(16 * n * x.shape[0] for n, x, _ in jobs)
+
+    def work(c):
+        n, x, y, r0, r1 = c
+        fn(x[r0:r1].ctypes.data, y[r0:r1].ctypes.data, n, r1 - r0)
+
+    t0 = time.perf_counter()
+    reps = 0
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while True:
+            list(ex.map(work, chunks))
+            reps += 1
+            if time.perf_counter() - t0 >= budget_s:
+                break
+    dt = time.perf_counter() - t0
+    desc = (f"grid49 with <= {rows_cap} rows per point ({nbytes / 1e6:.1f} MB algorithmic per pass), "
+            f"{reps} passes, {threads} threads, {'oracle/_ref refFftF32' if kind == 'reference' else 'C restatement'}")
+    return nbytes * reps / dt / 1e9, dt, nbytes * reps, kind, desc
+
+
+def stdlib_numpy_sample(budget_s: float):
+    """numpy.fft.fft on complex64 (the reference's stdlib baseline, scripts/bench_stdlib.py),
+    single-threaded pocketfft, on the grid capped at 64 rows per point."""
+    xs = []
+    for n in GRID_N:
+        for b in GRID_B:
+            rng = np.random.default_rng(grid_seed(n, b))
+            z = rng.standard_normal((min(b, 64), 2 * n)).astype(np.float32).view(np.complex64)
+            xs.append(z)
+    nbytes = sum(16 * z.size for z in xs)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        for z in xs:
+            np.fft.fft(z, axis=-1)
+        reps += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return nbytes * reps / dt / 1e9
+
+
+# ------------------------------------------------------------------ distributed helpers
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    per_step = []
+    bytes_step = 0
+    kind = desc = None
+    for i in range(args.warmup + args.steps):
+        gbs, dt, nb, kind, desc = cpu_reference_sample(256, 0.0, threads)
+        if i >= args.warmup:
+            per_step.append(dt)
+            bytes_step = nb
+    ms = statistics.mean(per_step) * 1e3
+    value = bytes_step / (ms / 1e3) / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": "rows per grid point capped at 256",
+                       "points": len(GRID_N) * len(GRID_B)},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": desc},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+    world, rank, local = dist_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    import bfly
+
+    ctx = bfly.Context()
+    rc = ctx.init(device=dev.index)
+    if rc:
+        raise SystemExit(f"Context.init failed: {rc}")
+    plan = ctx.make_plan()
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+
+    # resident inputs and outputs for every grid point
+    pts = []
+    for n in GRID_N:
+        for b in GRID_B:
+            g = torch.Generator(device=dev).manual_seed(grid_seed(n, b))
+            x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
+            pts.append((n, b, x, torch.empty_like(x)))
+    for n, b, x, y in pts:   # builds twiddle tables outside any capture
+        assert plan.prepare(n, b) == 0
+
+    def step():
+        for n, b, x, y in pts:
+            r = plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh)
+            if r:
+                raise RuntimeError(f"exec_c2c({n},{b}) = {r}")
+
+    # parity spot check of the product path before timing
+    with torch.cuda.stream(stream):
+        step()
+    stream.synchronize()
+    import oracle.fft_oracle as O
+    worst = 0.0
+    for n, b, x, y in pts:
+        rows = O.sample_batches(b, 2)
+        ref = np.fft.fft(x[rows].cpu().numpy().astype(np.complex128), axis=-1)
+        worst = max(worst, O.rel_l2_rows(y[rows].cpu().numpy(), ref))
+    assert worst <= 1e-6, f"parity check failed: rel L2 {worst}"
+
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        step()
+    launches_per_step = len(pts)
+
+    def replay():
+        with torch.cuda.stream(stream):
+            graph.replay()
+
+    for _ in range(max(3, args.warmup)):
+        replay()
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            replay()
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    torch.cuda.synchronize()
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+        dist.barrier()
+    total_bytes = grid_bytes() * world
+    value = total_bytes / (ms / 1e3) / 1e9
+
+    # roofline: the dominant launch timed alone on its stream
+    n, b = DOMINANT
+    xd = next(x for (nn, bb, x, y) in pts if (nn, bb) == DOMINANT)
+    yd = torch.empty_like(xd)
+    reps = 50
+    for _ in range(5):
+        plan.exec_c2c(xd.data_ptr(), yd.data_ptr(), n, b, -1, 1.0, sh)
+    stream.synchronize()
+    d0 = torch.cuda.Event(enable_timing=True)
+    d1 = torch.cuda.Event(enable_timing=True)
+    d0.record(stream)
+    for _ in range(reps):
+        plan.exec_c2c(xd.data_ptr(), yd.data_ptr(), n, b, -1, 1.0, sh)
+    d1.record(stream)
+    d1.synchronize()
+    dom_ms = d0.elapsed_time(d1) / reps
+    dom_bytes = 16 * n * b
+    peak, peak_kind = load_peaks()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+
+    # e2e through the C ABI with pinned host buffers: H2D + kernel + D2H per grid point
+    host = []
+    for (nn, bb, x, y) in pts:
+        hx = torch.empty((bb, 2 * nn), dtype=torch.float32, pin_memory=True)
+        hx.copy_(torch.view_as_real(x).reshape(bb, 2 * nn).cpu())
+        hy = torch.empty_like(hx).pin_memory()
+        host.append((nn, bb, hx.numpy(), hy.numpy()))
+    for nn, bb, hx, hy in host:   # warm-up (device buffers grow to the largest point)
+        assert plan.run(hx, hy, nn, bb) == 0
+    e2e_steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for nn, bb, hx, hy in host:
+            r = plan.run(hx, hy, nn, bb)
+            if r:
+                raise RuntimeError(f"run({nn},{bb}) = {r}")
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = t.item()
+    h2d = sum(8 * nn * bb for nn, bb, _, _ in host)
+    e2e_value = grid_bytes() * world / e2e_s / 1e9
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    cpu = None
+    if world == 1:
+        threads = os.cpu_count() or 1
+        gbs, dt, nb, kind, desc = cpu_reference_sample(256, 10.0, threads)
+        cpu = {"value": round(gbs, 4), "unit": UNIT, "cores": threads, "kind": kind, "sample": desc,
+               "stdlib_numpy_1core_gbs": round(stdlib_numpy_sample(3.0), 4)}
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "points": len(pts), "bytes_per_step": grid_bytes() * world,
+                   "l2": "355 MB in + 355 MB out per step > 126 MB L2; no flush",
+                   "launch": "49 launches per step replayed from one CUDA graph",
+                   "parallelism": f"batch-sharded replicas x{world}", "candidate": plan.candidate_id,
+                   "parity_rel_l2_max": worst},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": dominant_traffic(),
+                     "kernel": "k_c2c<4096,16,1,fwd> N=4096 batch=4096", "peak_kind": peak_kind,
+                     "launch_us": round(dom_ms * 1e3, 3), "algorithmic_bytes": dom_bytes},
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": h2d, "path": "bfly_plan_run_c2c, pinned host buffers"},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+        "frac_of_roofline_step": round(value / world / peak, 4),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_case(spec: str, reps: int):
+    """Launch one kernel configuration `reps` times without timing (for ncu captures):
+    spec = kind:n:batch with kind in c2c, c2c_inv, r2c, c2r."""
+    import torch
+    import bfly
+    kind, n, b = spec.split(":")
+    n, b = int(n), int(b)
+    dev = torch.device("cuda", 0)
+    ctx = bfly.Context()
+    assert ctx.init() == 0
+    plan = ctx.make_plan()
+    g = torch.Generator(device=dev).manual_seed(grid_seed(n, b))
+    if kind in ("c2c", "c2c_inv"):
+        x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.empty_like(x)
+        call = lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, 1 if kind == "c2c_inv" else -1, 1.0, 0)
+    elif kind == "r2c":
+        x = torch.randn(b, n, device=dev, generator=g)
+        y = torch.empty(b, n // 2 + 1, dtype=torch.complex64, device=dev)
+        call = lambda: plan.exec_r2c(x.data_ptr(), y.data_ptr(), n, b, 1.0, 1.0, 0)
+    elif kind == "c2r":
+        x = torch.randn(b, n // 2 + 1, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.empty(b, n, device=dev)
+        call = lambda: plan.exec_c2r(x.data_ptr(), y.data_ptr(), n, b, 1.0, 1.0, 1.0 / n, 0)
+    else:
+        raise SystemExit(f"unknown case kind {kind}")
+    for _ in range(reps):
+        r = call()
+        if r:
+            raise SystemExit(f"{spec}: status {r}")
+    torch.cuda.synchronize()
+    print(f"case {spec} x{reps} ok")
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default=None, help="kind:n:batch, launch only that kernel (for ncu)")
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args(argv)
+    if args.case:
+        return run_case(args.case, args.reps)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

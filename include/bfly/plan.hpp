@@ -120,6 +120,38 @@ public:
 };
 
 class Context;
+class Plan;
+
+// One request of a ragged launch: C2C of `batch` rows of length n (32..4096, power of two)
+// between device buffers, direction -1 forward / +1 inverse, output times scale.
+struct RaggedRequest {
+    const void* in;
+    void* out;
+    uint32_t n;
+    uint64_t batch;
+    int direction;
+    float scale;
+};
+
+// A device work list for one persistent launch over many requests of different lengths and
+// batch counts (built once; exec() is a single kernel launch, capturable in a CUDA graph).
+// Must not outlive the Plan that built it (it uses that plan's twiddle tables).
+class Ragged {
+public:
+    ~Ragged();
+    int exec(void* stream) const;
+    uint64_t tiles() const { return total_; }
+    int grid() const { return grid_; }
+    size_t requests() const { return count_; }
+
+private:
+    friend class Plan;
+    Ragged() = default;
+    void* entries_ = nullptr;
+    size_t count_ = 0;
+    uint64_t total_ = 0;
+    int grid_ = 0;
+};
 
 class Plan {
 public:
@@ -143,8 +175,9 @@ public:
     int runInverse(const float* in, float* out, uint32_t n, uint32_t batch, float scale);
     int runLong(const float* in, float* out, uint32_t n, uint32_t batch, int direction);
 
-    // Asynchronous device-pointer entry points: enqueue on `stream` (nullptr = the context
-    // stream) and return; no host synchronisation, no host<->device copies.
+    // Asynchronous device-pointer entry points: enqueue on `stream` (a cudaStream_t; nullptr is
+    // the CUDA default stream, stream() the context stream) and return; no host
+    // synchronisation, no host<->device copies.
     //   direction -1 forward, +1 inverse; scale multiplies the output.
     //   n in [32, 16384] single pass, [8192, 65536] four-step (workspace grown on demand).
     int execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
@@ -157,6 +190,10 @@ public:
     // (1/n = numpy.fft.irfft).
     int execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
                 float sInt, float outScale, void* stream);
+
+    // Build a ragged persistent launch over `count` requests; *status receives 0 or a code
+    // (-8 invalid request, -2 table build, -3 alloc, -4 upload, -1 runtime).
+    std::unique_ptr<Ragged> makeRagged(const RaggedRequest* reqs, size_t count, int* status);
 
     void* stream() const { return stream_; }
 

@@ -106,8 +106,9 @@ int bfly_plan_run_c2c_inverse(bfly_plan* plan, const float* in, float* out, uint
 int bfly_plan_run_c2c_long(bfly_plan* plan, const float* in, float* out, uint32_t n,
                            uint32_t batch, int direction);
 
-/* New asynchronous device-pointer entry points.  Enqueue on `stream` (cudaStream_t; NULL =
- * the context stream) and return without synchronising.  The first call for a length builds
+/* New asynchronous device-pointer entry points.  Enqueue on `stream` (a cudaStream_t; NULL is
+ * the CUDA default stream, bfly_context_stream() the context's) and return without
+ * synchronising.  The first call for a length builds
  * its twiddle tables (and the four-step workspace) and synchronises the context stream once;
  * make it before any stream capture. */
 /* C2C, n in [32, 65536]; direction -1 forward / +1 inverse; output multiplied by scale. */
@@ -122,6 +123,28 @@ int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uin
 int bfly_plan_exec_c2r_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, float s_edge, float s_int, float out_scale,
                              void* stream);
+
+/* New: ragged persistent launch.  One kernel launch transforms a set of requests with
+ * different lengths (32..4096, powers of two), batch counts and directions; the work list is
+ * built once on the device and exec is a single launch that can be captured in a CUDA graph.
+ * The ragged object uses the plan's twiddle tables and must be destroyed before the plan.
+ * The reference has no counterpart (it launches one kernel per transform,
+ * src/framework/butterfly.cpp:743). */
+typedef struct bfly_ragged bfly_ragged;
+typedef struct bfly_ragged_request {
+    const void* d_in;      /* [batch][n] complex64 */
+    void* d_out;           /* [batch][n] complex64 */
+    uint32_t n;
+    int32_t direction;     /* -1 forward, +1 inverse */
+    uint64_t batch;
+    float scale;
+    uint32_t reserved;
+} bfly_ragged_request;
+int bfly_ragged_create(bfly_plan* plan, const bfly_ragged_request* reqs, size_t count,
+                       bfly_ragged** out);
+int bfly_ragged_exec_async(bfly_ragged* ragged, void* stream);
+int bfly_ragged_info(bfly_ragged* ragged, uint64_t* tiles, int* grid);
+void bfly_ragged_destroy(bfly_ragged* ragged);
 
 /* Acceptance helpers with the reference's semantics (include/butterfly/reference.hpp:14-60). */
 double bfly_max_rel_scaled(const float* got, const float* ref, size_t len);

@@ -1,0 +1,159 @@
+// CPU fake of the device seam (ascend-fft_b200/csrc/backend.h) for host-runtime tests.
+// "Device memory" is host memory, copies are memcpy, kernels compute a direct DFT on the
+// host, and every call is counted with one-shot failure injection -- the pattern of the
+// reference's tests/stubs/acl/acl_rt.h:15-53.  Test infrastructure only.
+#include "backend.h"
+#include "ragged.h"
+
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+namespace fake {
+int allocations = 0, releases = 0, copies = 0, launches = 0, syncs = 0;
+int failAllocation = 0, failCopy = 0, failLaunch = 0, failSync = 0;   // 1-based call index
+int streamsCreated = 0, streamsDestroyed = 0;
+int deviceCountValue = 1;
+float timerMs = 0.01f;   // reported time per launch
+}  // namespace fake
+
+namespace bfly {
+namespace backend {
+
+namespace {
+using cd = std::complex<double>;
+
+// direct DFT of one row (sign -1 forward), host reference for the fake kernels
+void dft(const float* in, float* out, uint32_t n, int sign, float scale) {
+    std::vector<cd> x(n), y(n);
+    for (uint32_t i = 0; i < n; ++i) x[i] = cd(in[2 * i], in[2 * i + 1]);
+    for (uint32_t k = 0; k < n; ++k) {
+        cd acc = 0;
+        for (uint32_t j = 0; j < n; ++j) {
+            const double a = sign * 2.0 * M_PI * (double)(((uint64_t)j * k) % n) / (double)n;
+            acc += x[j] * cd(std::cos(a), std::sin(a));
+        }
+        y[k] = acc * (double)scale;
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+        out[2 * k] = (float)y[k].real();
+        out[2 * k + 1] = (float)y[k].imag();
+    }
+}
+
+int launch() {
+    ++fake::launches;
+    return fake::launches == fake::failLaunch ? 1 : 0;
+}
+bool known(int e, int cta, uint32_t n) {
+    if ((e != 8 && e != 16) || n < 2u * (uint32_t)e || (n & (n - 1))) return false;
+    const uint32_t T = n / (uint32_t)e;
+    return (cta == 128 || cta == 256 || cta == 512 || cta == 1024) && T <= (uint32_t)cta &&
+           (cta == 1024) == (T == 1024);
+}
+}  // namespace
+
+int deviceCount(int* count) { *count = fake::deviceCountValue; return 0; }
+int setDevice(int) { return 0; }
+int deviceName(int, char* buf, size_t cap) { std::strncpy(buf, "fake", cap); return 0; }
+int smCount(int, int* count) { *count = 148; return 0; }
+int streamCreate(void** s) { ++fake::streamsCreated; *s = reinterpret_cast<void*>(0x1); return 0; }
+int streamDestroy(void*) { ++fake::streamsDestroyed; return 0; }
+int alloc(void** p, size_t bytes) {
+    ++fake::allocations;
+    if (fake::allocations == fake::failAllocation) { *p = nullptr; return 2; }
+    *p = std::malloc(bytes ? bytes : 1);
+    return *p ? 0 : 2;
+}
+int release(void* p) { ++fake::releases; std::free(p); return 0; }
+int allocHost(void** p, size_t bytes) { *p = std::malloc(bytes); return *p ? 0 : 2; }
+int releaseHost(void* p) { std::free(p); return 0; }
+int copyH2D(void* dst, const void* src, size_t bytes, void*) {
+    ++fake::copies;
+    if (fake::copies == fake::failCopy || !dst || !src) return 1;
+    std::memcpy(dst, src, bytes);
+    return 0;
+}
+int copyD2H(void* dst, const void* src, size_t bytes, void* s) { return copyH2D(dst, src, bytes, s); }
+int streamSync(void*) {
+    ++fake::syncs;
+    return fake::syncs == fake::failSync ? 1 : 0;
+}
+
+struct Timer { int dummy; };
+int timerCreate(Timer** t) { *t = new Timer{0}; return 0; }
+int timerStart(Timer*, void*) { return 0; }
+int timerStop(Timer*, void*, float* ms) { *ms = fake::timerMs; return 0; }
+void timerDestroy(Timer* t) { delete t; }
+
+bool hasVariant(int kind, uint32_t n, int e, int cta) {
+    if (kind == kC2C) return n >= 32 && n <= 16384 && known(e, cta, n);
+    return n >= 64 && n <= 8192 && known(e, cta, n / 2);
+}
+size_t variantSmemBytes(int, uint32_t n, int, int) { return (size_t)n * 9; }
+
+size_t stockhamTwiddleCount(uint32_t n, int) { return n; }
+int buildStockhamTwiddles(void* tw, uint32_t n, int, void*) {
+    std::memset(tw, 0, (size_t)n * 8);
+    return launch();
+}
+int buildLinearTwiddles(void* tw, int count, long long, long long, void*) {
+    std::memset(tw, 0, (size_t)count * 8);
+    return launch();
+}
+
+int launchC2C(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+              const void*, int, int, void*) {
+    if (int r = launch()) return r;
+    for (uint64_t b = 0; b < batch; ++b)
+        dft((const float*)in + b * 2 * n, (float*)out + b * 2 * n, n, inverse ? 1 : -1, scale);
+    return 0;
+}
+int launchR2C(const void*, void*, uint32_t, uint64_t, const void*, const void*, int, int, bool,
+              float, float, void*) {
+    return launch();
+}
+int launchC2R(const void*, void*, uint32_t, uint64_t, const void*, const void*, int, int, float,
+              float, float, void*) {
+    return launch();
+}
+
+bool hasLongSplit(uint32_t n1, uint32_t n2) { return n1 >= 32 && n1 <= 256 && n2 == 256; }
+void longSplit(uint32_t n, uint32_t* n1, uint32_t* n2) {
+    *n1 = *n2 = 0;
+    if (n >= 8192 && n <= 65536 && !(n & (n - 1))) { *n2 = 256; *n1 = n / 256; }
+}
+int longE() { return 16; }
+int launchLongA(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t batch, bool,
+                const void*, const void*, const void*, void*) {
+    if (int r = launch()) return r;
+    std::memcpy(out, in, (size_t)n1 * n2 * batch * 8);
+    return 0;
+}
+int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t batch, bool inverse,
+                float scale, const void*, void*) {
+    if (int r = launch()) return r;
+    const uint32_t n = n1 * n2;
+    for (uint64_t b = 0; b < batch; ++b)
+        dft((const float*)in + b * 2 * n, (float*)out + b * 2 * n, n, inverse ? 1 : -1, scale);
+    return 0;
+}
+
+int raggedSmemBytes() { return 34816; }
+int raggedGrid(int, int* grid) { *grid = 148 * 2; return 0; }
+int launchRagged(const void* entries, int count, uint64_t, int, void*) {
+    if (int r = launch()) return r;
+    const RaggedEntry* es = static_cast<const RaggedEntry*>(entries);
+    for (int i = 0; i < count; ++i) {
+        const uint32_t n = 1u << es[i].logn;
+        for (uint64_t b = 0; b < es[i].batch; ++b)
+            dft((const float*)es[i].in + b * 2 * n, (float*)es[i].out + b * 2 * n, n, es[i].direction,
+                es[i].scale);
+    }
+    return 0;
+}
+
+}  // namespace backend
+}  // namespace bfly

@@ -1,0 +1,333 @@
+// CPU host-runtime tests against the fake device seam (fake_backend.cpp).  Ports the intent of
+// the reference's tests/test_runtime_guards.cpp: strict configuration loading, -9 re-init,
+// candidate mutations that have no lowering, guards that reject every illegal shape with zero
+// allocations / copies / launches, and failure injection proving a failed prepare never leaves
+// a stale key.  Adds the B200 runtime's own contracts: host round-trip error codes, measure and
+// select acceptance, and the persisted tuning cache.
+#include "bfly/plan.hpp"
+
+#include <cassert>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace fake {
+extern int allocations, releases, copies, launches, syncs;
+extern int failAllocation, failCopy, failLaunch, failSync;
+extern int streamsCreated, streamsDestroyed, deviceCountValue;
+extern float timerMs;
+}  // namespace fake
+
+#define CHECK(cond)                                                                    \
+    do {                                                                               \
+        if (!(cond)) {                                                                 \
+            std::fprintf(stderr, "CHECK failed at %s:%d: %s\n", __FILE__, __LINE__, #cond); \
+            std::exit(1);                                                              \
+        }                                                                              \
+    } while (0)
+
+static std::string read(const std::string& path) {
+    std::ifstream f(path);
+    return {std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>()};
+}
+static std::string replaced(std::string text, const std::string& from, const std::string& to) {
+    const size_t at = text.find(from);
+    CHECK(at != std::string::npos);
+    text.replace(at, from.size(), to);
+    return text;
+}
+static void write(const std::string& path, const std::string& text) {
+    std::ofstream f(path);
+    f << text;
+    CHECK(f.good());
+}
+static bool throws(const std::function<void()>& fn) {
+    try {
+        fn();
+    } catch (const std::exception&) {
+        return true;
+    }
+    return false;
+}
+
+int main(int argc, char** argv) {
+    CHECK(argc == 3);
+    const std::string cfg = argv[1], tmp = argv[2];
+    const std::string profile = cfg + "/b200_profile.json", space = cfg + "/b200_space.json";
+    const std::string hwText = read(profile), spText = read(space);
+    const std::string badHw = tmp + "/hw.json", badSp = tmp + "/space.json";
+
+    // ---- strict configuration (-4), no runtime touched
+    CHECK(throws([] { bfly::Hardware::load("/nonexistent-hardware-config"); }));
+    CHECK(throws([] { bfly::DesignSpace::load("/nonexistent-space-config"); }));
+    for (const auto& bad : {std::string("{}"), hwText + " trailing",
+                            replaced(hwText, "\"sm_count\": 148", "\"sm_count\": 0"),
+                            replaced(hwText, "\"sm_count\": 148", "\"sm_count\": \"148\""),
+                            replaced(hwText, "\"sm_count\": 148", "\"sm_count\": 148.5"),
+                            replaced(hwText, "\"hbm_gbs\": 6446.0", "\"hbm_gbs\": -1"),
+                            replaced(hwText, "\"schema_version\": 1", "\"schema_version\": 2"),
+                            replaced(hwText, "\"sm_count\": 148,", "\"sm_count\": 148, \"sm_count\": 1,")}) {
+        write(badHw, bad);
+        CHECK(throws([&] { bfly::Hardware::load(badHw); }));
+        bfly::Context invalid;
+        CHECK(invalid.init(badHw, space, "builtin") == -4);
+    }
+    for (const auto& bad : {std::string("{"), std::string("{}"), spText + " trailing",
+                            replaced(spText, "\"cta_threads\": [128, 256, 512]", "\"cta_threads\": []"),
+                            replaced(spText, "\"cta_threads\": [128, 256, 512]", "\"cta_threads\": [100]"),
+                            replaced(spText, "\"radix\": [8, 16]", "\"radix\": [\"8\"]"),
+                            replaced(spText, "\"radix\": [8, 16]", "\"radix\": [3]"),
+                            replaced(spText, "\"out\": [\"interleaved\", \"planar\"]", "\"out\": [\"bogus\"]"),
+                            replaced(spText, "\"schedule\": [\"stockham\", \"four_step\"]", "\"schedule\": [\"fast\"]")}) {
+        write(badSp, bad);
+        CHECK(throws([&] { bfly::DesignSpace::load(badSp); }));
+        bfly::Context invalid;
+        CHECK(invalid.init(profile, badSp, "builtin") == -4);
+    }
+    CHECK(fake::streamsCreated == 0);
+
+    // ---- runtime errors at init
+    {
+        fake::deviceCountValue = 0;
+        bfly::Context noDevice;
+        CHECK(noDevice.init(profile, space, "builtin") == -1);
+        fake::deviceCountValue = 1;
+        bfly::Context badDevice;
+        CHECK(badDevice.init(profile, space, "builtin", 3) == -2);
+    }
+
+    bfly::Context context;
+    CHECK(context.init(profile, space, "builtin") == 0);
+    CHECK(fake::streamsCreated == 1);
+    CHECK(context.init(profile, space, "builtin") == -9);
+    CHECK(fake::streamsCreated == 1);
+    CHECK(context.hardware().smCount == 148);
+
+    // ---- candidates and lowering
+    auto candidates = context.enumerate(64, 1);
+    std::unique_ptr<bfly::Plan> plan;
+    for (const auto& c : candidates)
+        if (c.state != bfly::State::Infeasible && c.p.radix == 16 && c.a.ctaThreads == 256) {
+            plan = context.makePlan(c);
+            break;
+        }
+    CHECK(plan);
+    const auto canonical = plan->candidate();
+    const std::vector<std::function<void(bfly::Candidate&)>> mutations = {
+        [](auto& c) { c.p.fusionLevel = 2; },
+        [](auto& c) { c.p.coefficientResidency = false; },
+        [](auto& c) { c.p.radix = 4; },
+        [](auto& c) { c.l.contiguous = false; },
+        [](auto& c) { c.l.in = bfly::Layout::Planar; },
+        [](auto& c) { c.l.out = bfly::Layout::Planar; },
+        [](auto& c) { c.a.level = 1; },
+        [](auto& c) { c.a.ctaThreads = 0; },
+        [](auto& c) { c.a.ctaThreads = 96; },
+        [](auto& c) { c.a.localExchange = "shuffle"; },
+        [](auto& c) { c.a.localExchange = "register"; },
+        [](auto& c) { c.f.precision = "split_bf16"; },
+        [](auto& c) { c.f.schedule = "bogus"; },
+        [](auto& c) { c.state = bfly::State::Infeasible; }};
+    for (const auto& mutate : mutations) {
+        auto c = canonical;
+        mutate(c);
+        CHECK(!context.makePlan(c));
+    }
+    bfly::Context uninitialized;
+    CHECK(!uninitialized.makePlan(canonical));
+    {
+        bfly::Context missingKernel;
+        CHECK(missingKernel.init(profile, space, tmp + "/does-not-exist.so") == 0);
+        CHECK(!missingKernel.makePlan(canonical));
+    }
+    int feasible = 0;
+    for (const auto& c : candidates) {
+        if (c.state != bfly::State::Infeasible) {
+            CHECK(context.makePlan(c));
+            ++feasible;
+        }
+        if (c.a.localExchange != "shared" || c.l.in != bfly::Layout::Interleaved ||
+            c.l.out != bfly::Layout::Interleaved)
+            CHECK(c.state == bfly::State::Infeasible && !c.reason.empty());
+        if (c.f.schedule == "four_step") CHECK(c.state == bfly::State::Infeasible);   // n <= 4096
+    }
+    CHECK(feasible > 0);
+
+    // infeasibility reasons carry a key
+    auto reasonFor = [&](uint32_t n, uint32_t batch) {
+        std::string all;
+        for (const auto& c : context.enumerate(n, batch)) {
+            CHECK(c.state == bfly::State::Infeasible);
+            all += c.reason + "\n";
+        }
+        return all;
+    };
+    CHECK(reasonFor(16, 64).find("minimum") != std::string::npos);
+    CHECK(reasonFor(72, 64).find("power of two") != std::string::npos);
+    CHECK(reasonFor(192, 64).find("power of two") != std::string::npos);
+    CHECK(reasonFor(131072, 1).find("envelope") != std::string::npos);
+    CHECK(reasonFor(64, 0).find("batch") != std::string::npos);
+    CHECK(reasonFor(4096, 524288).find("uint32") != std::string::npos);
+    {   // the uint32 offset boundary of the host-pointer API: 524287 live, 524288 rejected
+        bool live = false;
+        for (const auto& c : context.enumerate(4096, 524287)) live = live || c.state != bfly::State::Infeasible;
+        CHECK(live);
+    }
+    {   // long lengths: four-step feasible, single pass only up to 16384
+        int fs = 0, sp = 0;
+        for (const auto& c : context.enumerate(65536, 4))
+            if (c.state != bfly::State::Infeasible) (c.f.schedule == "four_step" ? fs : sp)++;
+        CHECK(fs == 1 && sp == 0);
+        bool single8192 = false;
+        for (const auto& c : context.enumerate(8192, 4))
+            single8192 = single8192 || (c.state != bfly::State::Infeasible && c.f.schedule == "stockham");
+        CHECK(single8192);
+    }
+
+    // ---- guards: -8 before any allocation, copy or launch
+    float dummy[4] = {0, 0, 0, 0};
+    for (uint32_t n : {0u, 1u, 32u, 192u, 16384u}) {
+        CHECK(plan->run(dummy, dummy, n, 1) == -8);
+        CHECK(plan->runR2C(dummy, dummy, n, 1) == -8);
+        CHECK(plan->runC2R(dummy, dummy, n, 1) == -8);
+    }
+    for (uint32_t n : {0u, 1u, 16u, 192u, 131072u}) CHECK(plan->prepare(n, 1) == -8);
+    CHECK(plan->run(dummy, dummy, 8192, 1) == -8);
+    CHECK(plan->runC2R(dummy, dummy, 8192, 1) == -8);
+    CHECK(plan->runR2C(dummy, dummy, 64, 1) == -8);
+    CHECK(plan->runLong(dummy, dummy, 4096, 1, -1) == -8);
+    CHECK(plan->runLong(dummy, dummy, 8192, 1, 0) == -8);
+    for (auto run : {&bfly::Plan::run, &bfly::Plan::runR2C, &bfly::Plan::runC2R}) {
+        CHECK((plan.get()->*run)(dummy, dummy, 128, 0) == -8);
+        CHECK((plan.get()->*run)(nullptr, dummy, 128, 1) == -8);
+        CHECK((plan.get()->*run)(dummy, nullptr, 128, 1) == -8);
+        CHECK((plan.get()->*run)(dummy, dummy, 128, 0xffffffffu) == -8);
+    }
+    CHECK(plan->execC2C(nullptr, dummy, 64, 1, -1, 1.f, nullptr) == -8);
+    CHECK(plan->execC2C(dummy, dummy, 64, 0, -1, 1.f, nullptr) == -8);
+    CHECK(plan->execC2C(dummy, dummy, 64, 1, 0, 1.f, nullptr) == -8);
+    CHECK(plan->execC2C(dummy, dummy, 96, 1, -1, 1.f, nullptr) == -8);
+    CHECK(plan->execC2C(dummy, dummy, 131072, 1, -1, 1.f, nullptr) == -8);
+    CHECK(plan->execR2C(dummy, dummy, 32, 1, 1.f, 1.f, nullptr) == -8);
+    CHECK(plan->execC2R(dummy, dummy, 16384, 1, 1.f, 1.f, 1.f, nullptr) == -8);
+    bfly::Metric metric;
+    CHECK(plan->measure(1, 1, &metric) == -8);
+    CHECK(plan->measure(64, 1, nullptr) == -1);
+    CHECK(plan->prepare(64, 0) == -8);
+    CHECK(fake::allocations == 0 && fake::copies == 0 && fake::launches == 0);
+
+    // ---- failure injection: a failed prepare never leaves a usable stale key
+    CHECK(plan->prepare(64, 1) == 0);
+    const int afterFirst = fake::allocations;
+    CHECK(afterFirst == 1);
+    fake::failAllocation = fake::allocations + 1;
+    CHECK(plan->prepare(128, 1) != 0);
+    fake::failAllocation = 0;
+    int before = fake::allocations;
+    CHECK(plan->prepare(128, 1) == 0);          // rebuilt, not served from a stale entry
+    CHECK(fake::allocations == before + 1);
+    fake::failLaunch = fake::launches + 1;      // twiddle build fails
+    CHECK(plan->prepare(256, 1) != 0);
+    fake::failLaunch = 0;
+    before = fake::allocations;
+    CHECK(plan->prepare(256, 1) == 0);
+    CHECK(fake::allocations == before + 1);
+    before = fake::allocations;
+    CHECK(plan->prepare(64, 1) == 0);            // cached
+    CHECK(plan->prepare(128, 1) == 0);
+    CHECK(fake::allocations == before);
+
+    // ---- host round trip: status code per failing step, correct values otherwise
+    const uint32_t n = 64, batch = 3;
+    std::vector<float> in(2 * n * batch), out(2 * n * batch), ref(2 * n);
+    for (size_t i = 0; i < in.size(); ++i) in[i] = bfly::patternAt(i);
+    CHECK(plan->run(in.data(), out.data(), n, batch) == 0);
+    for (uint32_t b = 0; b < batch; ++b) {
+        bfly::refFftF32(in.data() + b * 2 * n, ref.data(), n);
+        CHECK(bfly::maxRelScaled(out.data() + b * 2 * n, ref.data(), 2 * n) < 1e-5);
+    }
+    fake::failCopy = fake::copies + 1;
+    CHECK(plan->run(in.data(), out.data(), n, batch) == -4);
+    fake::failCopy = fake::copies + 2;
+    CHECK(plan->run(in.data(), out.data(), n, batch) == -7);
+    fake::failCopy = 0;
+    fake::failLaunch = fake::launches + 1;
+    CHECK(plan->run(in.data(), out.data(), n, batch) == -5);
+    fake::failLaunch = 0;
+    fake::failSync = fake::syncs + 1;
+    CHECK(plan->run(in.data(), out.data(), n, batch) == -6);
+    fake::failSync = 0;
+    fake::failAllocation = fake::allocations + 1;
+    CHECK(plan->run(in.data(), out.data(), 128, 4) == -3);   // larger buffers must grow
+    fake::failAllocation = 0;
+    CHECK(plan->run(in.data(), out.data(), n, batch) == 0);
+    CHECK(plan->runInverse(out.data(), out.data(), n, batch, 1.0f / n) == 0);
+    for (size_t i = 0; i < in.size(); ++i) CHECK(std::fabs(out[i] - in[i]) < 1e-5);
+
+    // ---- measure: acceptance against the FP64 check, state transitions
+    CHECK(plan->measure(64, 2, &metric) == 0);
+    CHECK(metric.measuredOk && metric.maxRelErr < 1e-5 && plan->candidate().state == bfly::State::Measured);
+    CHECK(std::fabs(metric.measuredUs - fake::timerMs * 1000.0) < 1e-6);
+
+    // ---- select + tuning cache
+    const std::string cache = tmp + "/tune.json";
+    context.setTuningCache(cache);
+    std::string log;
+    auto best = context.select(64, 2, 2, &log);
+    CHECK(best);
+    CHECK(log.find("accept") != std::string::npos && log.find("selected:") != std::string::npos);
+    CHECK(read(cache).find(best->candidate().id) != std::string::npos);
+    const int launchesBefore = fake::launches;
+    std::string log2;
+    auto cached = context.select(64, 2, 2, &log2);
+    CHECK(cached && cached->candidate().id == best->candidate().id);
+    CHECK(log2.find("tuning cache") != std::string::npos);
+    CHECK(fake::launches == launchesBefore);   // no measurement
+    write(cache, "{ not json");
+    std::string log3;
+    CHECK(context.select(64, 2, 1, &log3));    // corrupt cache ignored and rewritten
+    CHECK(read(cache).find("schema_version") != std::string::npos);
+
+    // ---- ragged work list: invalid requests rejected before allocation, values correct
+    {
+        std::vector<float> a(2 * 64 * 3), b(2 * 128 * 2), oa(a.size()), ob(b.size()), r(2 * 128);
+        for (size_t i = 0; i < a.size(); ++i) a[i] = bfly::patternAt(i);
+        for (size_t i = 0; i < b.size(); ++i) b[i] = bfly::patternAt(i + 7);
+        const int allocBefore = fake::allocations;
+        int st = 0;
+        bfly::RaggedRequest bad[] = {{a.data(), oa.data(), 96, 3, -1, 1.f}};
+        CHECK(!plan->makeRagged(bad, 1, &st) && st == -8);
+        bfly::RaggedRequest bad2[] = {{a.data(), oa.data(), 8192, 3, -1, 1.f}};
+        CHECK(!plan->makeRagged(bad2, 1, &st) && st == -8);
+        bfly::RaggedRequest bad3[] = {{a.data(), oa.data(), 64, 0, -1, 1.f}};
+        CHECK(!plan->makeRagged(bad3, 1, &st) && st == -8);
+        CHECK(!plan->makeRagged(nullptr, 1, &st) && st == -8);
+        CHECK(fake::allocations == allocBefore);
+        bfly::RaggedRequest ok[] = {{a.data(), oa.data(), 64, 3, -1, 1.f}, {b.data(), ob.data(), 128, 2, 1, 0.5f}};
+        auto rg = plan->makeRagged(ok, 2, &st);
+        CHECK(rg && st == 0 && rg->requests() == 2);
+        CHECK(rg->tiles() == 1 + 1);   // 64-point: 64 rows per tile; 128-point: 32 rows per tile
+        CHECK(rg->exec(nullptr) == 0);
+        for (uint32_t row = 0; row < 3; ++row) {
+            bfly::refFftF32(a.data() + row * 128, r.data(), 64);
+            CHECK(bfly::maxRelScaled(oa.data() + row * 128, r.data(), 128) < 1e-5);
+        }
+        fake::failAllocation = fake::allocations + 1;
+        CHECK(!plan->makeRagged(ok, 2, &st) && st == -3);
+        fake::failAllocation = 0;
+    }
+
+    plan.reset();
+    best.reset();
+    cached.reset();
+    CHECK(fake::releases > 0);
+    std::printf("host runtime guards: all checks passed (%d allocations, %d launches)\n",
+                fake::allocations, fake::launches);
+    return 0;
+}
