@@ -49,6 +49,8 @@ SIGNATURES = {
     "bfly_ragged_exec_async": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfly_ragged_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),
     "bfly_ragged_destroy": (None, [C.c_void_p]),
+    "bfly_exec_c2c_long_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
+                                             C.c_int, C.c_float, C.c_void_p]),
     "bfly_max_rel_scaled": (C.c_double, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "bfly_pattern_at": (C.c_float, [C.c_size_t]),
     "bfly_sample_batches": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]),

@@ -146,6 +146,20 @@ int bfly_ragged_exec_async(bfly_ragged* ragged, void* stream);
 int bfly_ragged_info(bfly_ragged* ragged, uint64_t* tiles, int* grid);
 void bfly_ragged_destroy(bfly_ragged* ragged);
 
+/* New: long C2C (four-step, n in {8192, 16384, 32768, 65536}) that allocates no device memory,
+ * for callers that cannot call cudaMalloc when they need the transform: code running while a
+ * CUDA graph is captured, real-time loops that must not allocate after start-up, programs whose
+ * GPU memory belongs to another allocator or budget.  No counterpart in the reference.
+ * Its workspace is a fixed 32 MiB array in the library's device image (every GPU that loads
+ * the library keeps it until exit), so n * batch must be <= 4,194,304 complex values; larger
+ * requests return -12 before any GPU work.  No plan or context is needed: it runs on the
+ * current device.  The first call on a device looks up the array addresses, builds its twiddle
+ * tables on `stream` and waits for that stream once; make that first call before any stream
+ * capture.  All calls share the one workspace: calls that overlap on the GPU race.
+ * Status: 0, -8 shape/direction, -10 null pointer, -12 too large, -1 runtime, -5 launch. */
+int bfly_exec_c2c_long_noalloc(const void* d_in, void* d_out, uint32_t n, uint64_t batch,
+                               int direction, float scale, void* stream);
+
 /* Acceptance helpers with the reference's semantics (include/butterfly/reference.hpp:14-60). */
 double bfly_max_rel_scaled(const float* got, const float* ref, size_t len);
 float bfly_pattern_at(size_t i);
