@@ -159,6 +159,19 @@ class Plan:
         return self._lib.bfly_plan_exec_c2r_async(self._h, d_in, d_out, n, batch, s_edge, s_int,
                                                   out_scale, stream or None)
 
+    def exec_c2c_tc(self, d_in: int, d_out: int, n: int, batch: int, direction: int = -1,
+                    scale: float = 1.0, split_terms: int = 3, stream: int = 0) -> int:
+        """Split-BF16 tensor-core C2C (n = 256 or 4096; 2 or 3 bf16 terms)."""
+        return self._lib.bfly_plan_exec_c2c_tc_async(self._h, d_in, d_out, n, batch, direction, scale,
+                                                     split_terms, stream or None)
+
+    def tc_device_status(self) -> int:
+        st = C.c_uint()
+        rc = self._lib.bfly_tc_device_status(C.byref(st))
+        if rc:
+            raise BflyError("bfly_tc_device_status", rc)
+        return st.value
+
     def make_ragged(self, requests):
         """requests: iterable of (d_in, d_out, n, batch, direction, scale) with device
         pointers; returns a Ragged whose exec(stream) is one persistent kernel launch."""
@@ -198,8 +211,17 @@ class Ragged:
     def info(self):
         tiles = C.c_uint64()
         grid = C.c_int()
-        self._lib.bfly_ragged_info(self._h, C.byref(tiles), C.byref(grid))
-        return {"tiles": tiles.value, "grid": grid.value}
+        stages = C.c_int()
+        self._lib.bfly_ragged_info(self._h, C.byref(tiles), C.byref(grid), C.byref(stages))
+        return {"tiles": tiles.value, "grid": grid.value, "stages": stages.value}
+
+    def device_status(self) -> int:
+        """0, or 1 when a staged launch gave up on a bounded wait (reading clears it)."""
+        st = C.c_uint()
+        rc = self._lib.bfly_ragged_device_status(C.byref(st))
+        if rc:
+            raise BflyError("bfly_ragged_device_status", rc)
+        return st.value
 
     def close(self):
         if getattr(self, "_h", None):

@@ -68,6 +68,23 @@ int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
 int raggedSmemBytes();
 int raggedGrid(int device, int* grid);   // resident CTAs on the whole device
 int launchRagged(const void* entries, int count, uint64_t totalTiles, int grid, void* stream);
+// TMA-staged variant (inputs 16-byte aligned): `stages` = 1 or 2 staging buffers per CTA.
+int raggedStagedGrid(int device, int stages, int* grid);
+int launchRaggedStaged(const void* entries, int count, uint64_t totalTiles, int grid, int stages,
+                       void* stream);
+// One tile per CTA (grid = tiles), hardware-scheduled; tileMap = request index per tile or
+// nullptr (binary search).
+int launchRaggedFlat(const void* entries, int count, const void* tileMap, uint64_t totalTiles,
+                     void* stream);
+// Device status word of the staged launches (nonzero: a bounded wait ran out).
+int raggedStatus(unsigned* status, bool clear);
+
+// Split-BF16 tensor-core C2C (tcgen05): n in {256, 4096}, split = 2 or 3 bf16 terms; tw is the
+// Stockham table of (n, 16).
+bool hasTensorVariant(uint32_t n, int split);
+int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+                    const void* tw, int split, void* stream);
+int tensorStatus(unsigned* status, bool clear);
 
 }  // namespace backend
 }  // namespace bfly

@@ -180,6 +180,15 @@ int bfly_plan_exec_c2r_async(bfly_plan* plan, const void* d_in, void* d_out, uin
     return p.execC2R(d_in, d_out, n, batch, s_edge, s_int, out_scale, stream);
 }
 
+int bfly_plan_exec_c2c_tc_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
+                                uint64_t batch, int direction, float scale, int split_terms,
+                                void* stream) {
+    PLAN_OR_FAIL();
+    return p.execC2CTensor(d_in, d_out, n, batch, direction, scale, split_terms, stream);
+}
+
+int bfly_tc_device_status(unsigned* status) { return bfly::Plan::tensorStatus(status); }
+
 int bfly_ragged_create(bfly_plan* plan, const bfly_ragged_request* reqs, size_t count,
                        bfly_ragged** out) {
     if (!plan || !plan->plan || !out) return -10;
@@ -200,12 +209,15 @@ int bfly_ragged_exec_async(bfly_ragged* ragged, void* stream) {
     return ragged->ragged->exec(stream);
 }
 
-int bfly_ragged_info(bfly_ragged* ragged, uint64_t* tiles, int* grid) {
+int bfly_ragged_info(bfly_ragged* ragged, uint64_t* tiles, int* grid, int* stages) {
     if (!ragged || !ragged->ragged) return -10;
     if (tiles) *tiles = ragged->ragged->tiles();
     if (grid) *grid = ragged->ragged->grid();
+    if (stages) *stages = ragged->ragged->stages();
     return 0;
 }
+
+int bfly_ragged_device_status(unsigned* status) { return bfly::Ragged::deviceStatus(status); }
 
 void bfly_ragged_destroy(bfly_ragged* ragged) { delete ragged; }
 

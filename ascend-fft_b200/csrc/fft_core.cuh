@@ -161,11 +161,15 @@ struct Sched {
         return (p < P - 1) ? E : (1 << (LOGN - (P - 1) * LOGE));
     }
     __host__ __device__ static constexpr int ns(int p) {  // product of radices before p
-        return p == 0 ? 1 : ns(p - 1) * radix(p - 1);
+        int v = 1;
+        for (int q = 0; q < p; ++q) v *= radix(q);
+        return v;
     }
     // float2 offset of pass p's twiddles in the table: (R_p - 1) * Ns_p entries per pass p >= 1
     __host__ __device__ static constexpr int twoff(int p) {
-        return p <= 1 ? 0 : twoff(p - 1) + (radix(p - 1) - 1) * ns(p - 1);
+        int off = 0;
+        for (int q = 1; q < p; ++q) off += (radix(q) - 1) * ns(q);
+        return off;
     }
     static constexpr int TWSIZE = twoff(P);
 };
@@ -188,23 +192,44 @@ __host__ __device__ constexpr int smem_stride() {
     else return base;
 }
 
+// ------------------------------------------------------------------ synchronisation
+// How the threads of one transform synchronise between passes:
+//   kSyncWarp   the transform lives inside one warp (T <= 32)
+//   kSyncNamed  the transform spans whole warps of a larger CTA: named barrier 1 + row, T threads
+//   kSyncBlock  the transform is the whole CTA
+enum SyncKind { kSyncWarp = 0, kSyncNamed = 1, kSyncBlock = 2 };
+
+template <int SYNC>
+__device__ __forceinline__ void team_sync(int row, int nthreads) {
+    if constexpr (SYNC == kSyncWarp) {
+        __syncwarp();
+    } else if constexpr (SYNC == kSyncNamed) {
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + row), "r"(nthreads) : "memory");
+    } else {
+        __syncthreads();
+    }
+}
+
+// Sync policy for a transform of T threads in a CTA of `ctaThreads`.
+__host__ __device__ constexpr int sync_kind(int T, int ctaThreads) {
+    return T <= 32 ? kSyncWarp : (T < ctaThreads ? kSyncNamed : kSyncBlock);
+}
+
 // ------------------------------------------------------------------ team FFT
 // One transform of length N held by T = N/E threads, E complex values per thread.
 // Thread t, slot s (< E/R), element r of pass p covers butterfly j = t + s*T.
 // On return, v[s*R_last + r] holds output element t + s*T + r*(N/R_last) (natural order).
 // `sm` is this transform's exchange buffer (smem_stride<> float2), `tw` the Stockham
 // twiddle table of Sched<N,E> (TWSIZE entries, pass p at twoff(p)), `load(i)` yields input
-// element i.  BLOCK_SYNC selects __syncthreads (transform spans warps) or __syncwarp.
-template <int N, int E, bool INV, bool BLOCK_SYNC>
+// element i.  SYNC selects the barrier (see team_sync); `row` is the transform's index in its
+// CTA (named-barrier id - 1).
+template <int N, int E, bool INV, int SYNC>
 struct Team {
     using S = Sched<N, E>;
     static constexpr int T = S::T;
     static constexpr int P = S::P;
 
-    static __device__ __forceinline__ void sync() {
-        if constexpr (BLOCK_SYNC) __syncthreads();
-        else __syncwarp();
-    }
+    static __device__ __forceinline__ void sync(int row) { team_sync<SYNC>(row, T); }
 
     template <class Load>
     static __device__ __forceinline__ void load_first(float2 (&v)[E], int t, Load&& load) {
@@ -218,7 +243,7 @@ struct Team {
 
     template <int p>
     static __device__ __forceinline__ void passes(float2 (&v)[E], float2* sm,
-                                                  const float2* __restrict__ tw, int t) {
+                                                  const float2* __restrict__ tw, int t, int row) {
         constexpr int R = S::radix(p);
         constexpr int B = E / R;
         constexpr int Ns = S::ns(p);
@@ -243,15 +268,15 @@ struct Team {
 #pragma unroll
                 for (int r = 0; r < R; ++r) sm[spad(base + r * Ns)] = v[s * R + r];
             }
-            sync();
+            sync(row);
             constexpr int R2 = S::radix(p + 1);
             constexpr int B2 = E / R2;
 #pragma unroll
             for (int s = 0; s < B2; ++s)
 #pragma unroll
                 for (int r = 0; r < R2; ++r) v[s * R2 + r] = sm[spad(t + s * T + r * (N / R2))];
-            if constexpr (p + 1 < P - 1) sync();   // next pass writes the buffer again
-            passes<p + 1>(v, sm, tw, t);
+            if constexpr (p + 1 < P - 1) sync(row);   // next pass writes the buffer again
+            passes<p + 1>(v, sm, tw, t, row);
         }
     }
 
@@ -263,9 +288,10 @@ struct Team {
 
     template <class Load>
     static __device__ __forceinline__ void run(float2 (&v)[E], float2* sm,
-                                               const float2* __restrict__ tw, int t, Load&& load) {
+                                               const float2* __restrict__ tw, int t, int row,
+                                               Load&& load) {
         load_first(v, t, load);
-        passes<0>(v, sm, tw, t);
+        passes<0>(v, sm, tw, t, row);
     }
 
     // Apply f(index, value) to every output element held by this thread.

@@ -31,7 +31,7 @@ k_c2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
       uint64_t batch, float scale) {
     constexpr int T = N / E;
     constexpr int S = smem_stride<N, E, false>();
-    using TM = Team<N, E, INV, (T > 32)>;
+    using TM = Team<N, E, INV, sync_kind(T, T * ROWS)>;
     extern __shared__ float2 smem[];
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
@@ -40,7 +40,7 @@ k_c2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     const float2* src = in + row * N;
     float2* dst = out + row * N;
     float2 v[E];
-    TM::run(v, smem + rl * S, tw, t,
+    TM::run(v, smem + rl * S, tw, t, rl,
             [&](int i) { return ok ? ld_stream(src + i) : make_float2(0.f, 0.f); });
     if (ok) TM::for_each_out(v, t, [&](int i, float2 x) { st_stream(dst + i, cscale(x, scale)); });
 }
@@ -58,7 +58,7 @@ k_r2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     constexpr int M = N / 2;
     constexpr int T = M / E;
     constexpr int S = smem_stride<M, E, false>();
-    using TM = Team<M, E, false, (T > 32)>;
+    using TM = Team<M, E, false, sync_kind(T, T * ROWS)>;
     extern __shared__ float2 smem[];
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
@@ -68,10 +68,10 @@ k_r2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     float2* dst = out + row * (M + 1);
     float2* sm = smem + rl * S;
     float2 v[E];
-    TM::run(v, sm, tw, t, [&](int i) { return ok ? ld_stream(src + i) : make_float2(0.f, 0.f); });
-    TM::sync();
+    TM::run(v, sm, tw, t, rl, [&](int i) { return ok ? ld_stream(src + i) : make_float2(0.f, 0.f); });
+    TM::sync(rl);
     TM::for_each_out(v, t, [&](int i, float2 x) { sm[spad(i)] = x; });
-    TM::sync();
+    TM::sync(rl);
     if (!ok) return;
     for (int k = t; k <= M; k += T) {
         const float2 a = sm[spad(k & (M - 1))];
@@ -97,7 +97,7 @@ k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     constexpr int M = N / 2;
     constexpr int T = M / E;
     constexpr int S = smem_stride<M, E, false>();
-    using TM = Team<M, E, true, (T > 32)>;
+    using TM = Team<M, E, true, sync_kind(T, T * ROWS)>;
     extern __shared__ float2 smem[];
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
@@ -106,7 +106,7 @@ k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     const float2* src = in + row * (M + 1);
     float2* dst = out + row * M;
     float2 v[E];
-    TM::run(v, smem + rl * S, tw, t, [&](int k) {
+    TM::run(v, smem + rl * S, tw, t, rl, [&](int k) {
         if (!ok) return make_float2(0.f, 0.f);
         float2 xk = __ldg(src + k), xm = __ldg(src + (M - k));
         if (k == 0) {
@@ -136,7 +136,7 @@ k_long_a(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
          const float2* __restrict__ tlo, const float2* __restrict__ thi, uint64_t batch, int logN2) {
     constexpr int T = N1 / E;
     constexpr int S = smem_stride<N1, E, true>();
-    using TM = Team<N1, E, INV, true>;
+    using TM = Team<N1, E, INV, kSyncBlock>;
     extern __shared__ float2 smem[];
     const int c = threadIdx.x % C;
     const int t = threadIdx.x / C;
@@ -149,7 +149,7 @@ k_long_a(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
     float2* dst = out + b * N + n2;
     (void)batch;
     float2 v[E];
-    TM::run(v, smem + c * S, tw, t, [&](int i) { return ld_stream(src + ((size_t)i << logN2)); });
+    TM::run(v, smem + c * S, tw, t, 0, [&](int i) { return ld_stream(src + ((size_t)i << logN2)); });
     TM::for_each_out(v, t, [&](int k1, float2 x) {
         const uint32_t m = n2 * (uint32_t)k1;
         const float2 w = cmul<false>(__ldg(thi + (m >> 8)), __ldg(tlo + (m & 255u)));
@@ -165,7 +165,7 @@ k_long_b(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
          uint64_t batch, int logN1, float scale) {
     constexpr int T = N2 / E;
     constexpr int S = smem_stride<N2, E, false>();
-    using TM = Team<N2, E, INV, (T > 32)>;
+    using TM = Team<N2, E, INV, sync_kind(T, T * C)>;
     extern __shared__ float2 smem[];
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
@@ -178,7 +178,7 @@ k_long_b(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
     float2* sm = smem + rl * S;
     (void)batch;
     float2 v[E];
-    TM::run(v, sm, tw, t, [&](int i) { return ld_stream(src + i); });
+    TM::run(v, sm, tw, t, rl, [&](int i) { return ld_stream(src + i); });
     __syncthreads();
     TM::for_each_out(v, t, [&](int i, float2 x) { sm[spad(i)] = x; });
     __syncthreads();

@@ -1,0 +1,264 @@
+// Split-BF16 tensor-core C2C for lengths that are powers of 16 (256, 4096): every radix-16 pass
+// is a dense complex contraction on the 5th-generation tensor cores.
+//
+// Pass structure (Stockham, as in fft_core.cuh, one butterfly per thread): thread t owns
+// butterfly j of its row and holds the 16 (twiddled, fp32) inputs x_0..x_15.  As reals they form
+// row t of an A operand (M = 128 butterflies per tile, K = 32: Re x_0..15, Im x_0..15).  The
+// 32 x 32 real matrix of DFT-16 is the B operand (K-major, N = 32 outputs: Re y_0..15,
+// Im y_0..15).  Both are split into bf16 terms, a = a_hi + a_lo (+ a_mid for three terms), and
+// D = sum over term pairs A_s * B_t accumulates in fp32 in tensor memory (two terms: 3 products
+// hi*hi + hi*lo + lo*hi; three terms: 6 products down to 2^-24).  tcgen05.ld returns D's row
+// t -- the 16 outputs of butterfly t -- to thread t, which writes them to the Stockham
+// positions of the next pass (or, after the last pass, to global memory).
+// Twiddles between passes stay fp32 (the Stockham tables of the CUDA-core path, E = 16).
+// Inverse transforms use IDFT(x) = conj(DFT(conj x)).
+#include "fft_kernels.cuh"
+#include "registry.cuh"
+#include "tcgen05.cuh"
+
+#include <cuda_bf16.h>
+
+namespace bfly {
+namespace dev {
+
+__device__ unsigned int g_tc_status;   // nonzero: a bounded wait for an MMA ran out
+
+constexpr int kTcThreads = 256;
+constexpr int kTileBytes = 128 * 32 * 2;   // one A tile: 128 rows x 32 bf16
+constexpr int kBBytes = 32 * 32 * 2;       // one B term: 32 rows x 32 bf16
+
+// Byte offset of element (row, k) in a no-swizzle K-major operand with K = 32: 8-row x 8-element
+// core matrices of 128 bytes, LBO = 128 (next 8 k), SBO = 512 (next 8 rows).
+__host__ __device__ constexpr uint32_t kmajor_offset(int row, int k) {
+    return (uint32_t)((row >> 3) * 512 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
+           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
+}
+
+// Split v into SPLIT bf16-representable terms (returned as floats, largest first).
+template <int SPLIT>
+__device__ __forceinline__ void split_terms(float v, float (&t)[SPLIT]) {
+    float r = v;
+#pragma unroll
+    for (int s = 0; s < SPLIT; ++s) {
+        t[s] = __bfloat162float(__float2bfloat16_rn(r));
+        r = r - t[s];
+    }
+}
+
+template <int N, int SPLIT>
+__global__ void __launch_bounds__(kTcThreads, SPLIT == 2 ? 3 : 2)
+k_c2c_tc(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
+         uint64_t batch, int direction, float scale) {
+    constexpr int E = 16;
+    using Sd = Sched<N, E>;
+    static_assert(Sd::radix(Sd::P - 1) == 16, "length must be a power of 16");
+    constexpr int T = N / E;                      // butterflies per row = threads per row
+    constexpr int ROWS = kTcThreads / T;
+    constexpr int S = smem_stride<N, E, false>();
+    constexpr int P = Sd::P;
+    constexpr int NPROD = SPLIT == 2 ? 3 : 6;
+
+    extern __shared__ __align__(1024) unsigned char smem_tc[];
+    unsigned char* aBase = smem_tc;                                 // [SPLIT][2 tiles][8 KB]
+    unsigned char* bBase = smem_tc + SPLIT * 2 * kTileBytes;          // [SPLIT][2 KB]
+    float2* xbuf = reinterpret_cast<float2*>(bBase + SPLIT * kBBytes);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(xbuf + ROWS * S);
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(bar + 1);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    if (warp == 0) {
+        tmem_alloc(tmemSlot, 64);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    // B terms: the 32 x 32 real DFT-16 matrix (forward), row n = output, column k = input.
+    //   Re y_n = sum_k c_nk Re x_k + s_nk Im x_k,  Im y_n = sum_k -s_nk Re x_k + c_nk Im x_k,
+    //   c_nk = cos(2 pi n k / 16), s_nk = sin(2 pi n k / 16)
+    for (int e = tid; e < 32 * 32; e += kTcThreads) {
+        const int n = e >> 5, k = e & 31;
+        const int nn = n & 15, kk = k & 15;
+        double sn, cs;
+        sincospi((double)((nn * kk) & 15) / 8.0, &sn, &cs);   // angles are multiples of pi/8
+        const float v = (float)((n < 16) ? (k < 16 ? cs : sn) : (k < 16 ? -sn : cs));
+        float parts[SPLIT];
+        split_terms<SPLIT>(v, parts);
+#pragma unroll
+        for (int s = 0; s < SPLIT; ++s)
+            *reinterpret_cast<__nv_bfloat16*>(bBase + s * kBBytes + kmajor_offset(n, k)) =
+                __float2bfloat16_rn(parts[s]);
+    }
+    fence_proxy_async_smem();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tmem = *tmemSlot;
+
+    const int rl = tid / T;
+    const int j = tid - rl * T;
+    const uint64_t row = (uint64_t)blockIdx.x * ROWS + rl;
+    const bool ok = row < batch;
+    const float sgn = direction > 0 ? -1.f : 1.f;
+    const int tile = tid >> 7, m = tid & 127;
+    const float2* src = in + row * N;
+    float2* dst = out + row * N;
+    float2* xr = xbuf + rl * S;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        float2 x = ok ? ld_stream(src + j + r * (N / 16)) : make_float2(0.f, 0.f);
+        v[r] = make_float2(x.x, sgn * x.y);
+    }
+    constexpr uint32_t idesc = umma_idesc_bf16(128, 32);
+    bool failed = false;
+    uint32_t pendingParity = 0;
+#pragma unroll 1
+    for (int p = 0; p < P; ++p) {
+        const int Ns = Sd::ns(p);
+        if (p > 0) {
+            const float2* twp = tw + Sd::twoff(p);
+            const int k = j & (Ns - 1);
+#pragma unroll
+            for (int r = 1; r < 16; ++r) v[r] = cmul<false>(v[r], __ldg(twp + (r - 1) * Ns + k));
+        }
+        // A terms of this butterfly: row m of tile `tile`, K chunks of 8 (Re 0-7, Re 8-15, Im 0-7, Im 8-15)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float pr[8][SPLIT];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int r = (c & 1) * 8 + e;
+                split_terms<SPLIT>(c < 2 ? v[r].x : v[r].y, pr[e]);
+            }
+#pragma unroll
+            for (int s = 0; s < SPLIT; ++s) {
+                uint4 q;
+                q.x = pack_bf16(pr[0][s], pr[1][s]);
+                q.y = pack_bf16(pr[2][s], pr[3][s]);
+                q.z = pack_bf16(pr[4][s], pr[5][s]);
+                q.w = pack_bf16(pr[6][s], pr[7][s]);
+                *reinterpret_cast<uint4*>(aBase + (s * 2 + tile) * kTileBytes + kmajor_offset(m, c * 8)) = q;
+            }
+        }
+        fence_proxy_async_smem();
+        tc_fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after_sync();
+            // products (A term, B term), smallest first
+            constexpr int pa[6] = {2, 1, 0, 1, 0, 0};
+            constexpr int pb[6] = {0, 1, 2, 0, 1, 0};
+            constexpr int pa2[3] = {1, 0, 0};
+            constexpr int pb2[3] = {0, 1, 0};
+#pragma unroll
+            for (int tl = 0; tl < 2; ++tl) {
+#pragma unroll
+                for (int q = 0; q < NPROD; ++q) {
+                    const int sa = SPLIT == 2 ? pa2[q] : pa[q];
+                    const int sb = SPLIT == 2 ? pb2[q] : pb[q];
+#pragma unroll
+                    for (int ks = 0; ks < 2; ++ks) {
+                        const uint32_t aAddr = smem_addr(aBase + (sa * 2 + tl) * kTileBytes) + ks * 256;
+                        const uint32_t bAddr = smem_addr(bBase + sb * kBBytes) + ks * 256;
+                        umma_bf16(tmem + tl * 32, umma_smem_desc(aAddr, 128, 512), umma_smem_desc(bAddr, 128, 512),
+                                  idesc, q > 0 || ks > 0);
+                    }
+                }
+            }
+            umma_commit(bar);
+        }
+        const bool done = mbar_wait_bounded(bar, (uint32_t)(p & 1));
+        if (__syncthreads_or(!done)) {
+            failed = true;
+            pendingParity = (uint32_t)(p & 1);
+            break;
+        }
+        tc_fence_after_sync();
+        float d[32];
+        tmem_ld_32cols(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(tile * 32), d);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = make_float2(d[r], d[16 + r]);
+        if (p < P - 1) {
+            const int k = j & (Ns - 1);
+            const int base = (j - k) * 16 + k;
+#pragma unroll
+            for (int r = 0; r < 16; ++r) xr[spad(base + r * Ns)] = v[r];
+            tc_fence_before_sync();
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = xr[spad(j + r * (N / 16))];
+        }
+    }
+    if (failed) {
+        if (tid == 0) {
+            atomicOr(&g_tc_status, 1u);
+            mbar_wait_bounded(bar, pendingParity);   // let the MMAs in flight finish if they can
+        }
+    } else if (ok) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r)
+            st_stream(dst + j + r * (N / 16), make_float2(v[r].x * scale, sgn * scale * v[r].y));
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 64);
+}
+
+template <int N, int SPLIT>
+constexpr int tcSmemBytes() {
+    return SPLIT * 2 * kTileBytes + SPLIT * kBBytes +
+           (kTcThreads / (N / 16)) * smem_stride<N, 16, false>() * 8 + 16;
+}
+
+}  // namespace dev
+
+namespace backend {
+
+template <int N, int SPLIT>
+static int launchTc(const void* in, void* out, uint64_t batch, bool inverse, float scale, const void* tw,
+                    void* stream) {
+    constexpr int smem = dev::tcSmemBytes<N, SPLIT>();
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(dev::k_c2c_tc<N, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess)
+            return 1;
+        attr = true;
+    }
+    constexpr int rows = dev::kTcThreads / (N / 16);
+    const unsigned grid = (unsigned)((batch + rows - 1) / rows);
+    dev::k_c2c_tc<N, SPLIT><<<grid, dev::kTcThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw), batch,
+        inverse ? 1 : -1, scale);
+    return (int)cudaGetLastError();
+}
+
+bool hasTensorVariant(uint32_t n, int split) { return (n == 256 || n == 4096) && (split == 2 || split == 3); }
+
+int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+                    const void* tw, int split, void* stream) {
+    if (n == 256 && split == 2) return launchTc<256, 2>(in, out, batch, inverse, scale, tw, stream);
+    if (n == 256 && split == 3) return launchTc<256, 3>(in, out, batch, inverse, scale, tw, stream);
+    if (n == 4096 && split == 2) return launchTc<4096, 2>(in, out, batch, inverse, scale, tw, stream);
+    if (n == 4096 && split == 3) return launchTc<4096, 3>(in, out, batch, inverse, scale, tw, stream);
+    return (int)cudaErrorInvalidValue;
+}
+
+int tensorStatus(unsigned* status, bool clear) {
+    if (cudaMemcpyFromSymbol(status, dev::g_tc_status, sizeof(unsigned)) != cudaSuccess) return 1;
+    if (clear && *status) {
+        const unsigned zero = 0;
+        if (cudaMemcpyToSymbol(dev::g_tc_status, &zero, sizeof(unsigned)) != cudaSuccess) return 1;
+    }
+    return 0;
+}
+
+}  // namespace backend
+}  // namespace bfly

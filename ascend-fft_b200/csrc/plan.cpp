@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -339,6 +340,7 @@ struct Plan::Impl {
     void* devWork = nullptr;
     size_t devInCap = 0, devOutCap = 0, devWorkCap = 0;
     backend::Timer* timer = nullptr;
+    void* aux[2] = {nullptr, nullptr};   // extra streams of the pipelined host round trip
 };
 
 Plan::Plan(Candidate c) : cand_(std::move(c)) {}
@@ -355,6 +357,8 @@ Plan::~Plan() {
     if (impl_->devOut) backend::release(impl_->devOut);
     if (impl_->devWork) backend::release(impl_->devWork);
     backend::timerDestroy(impl_->timer);
+    for (void* st : impl_->aux)
+        if (st) backend::streamDestroy(st);
 }
 
 static int ensureBuf(void** p, size_t* cap, size_t bytes) {
@@ -490,6 +494,12 @@ int Plan::prepare(uint32_t n, uint32_t batch) {
 
 int Plan::execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                   float scale, void* stream) {
+    return execC2CWith(dIn, dOut, n, batch, direction, scale, stream, nullptr);
+}
+
+// `work`: four-step workspace of n*batch complex values, or nullptr for the plan-owned one.
+int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
+                      float scale, void* stream, void* work) {
     if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull || (direction != -1 && direction != 1))
         return -8;
     if (!validShape(n, (uint32_t)batch, kExecC2C)) return -8;
@@ -505,14 +515,34 @@ int Plan::execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int d
     if (prepareLong(n)) return -2;
     uint32_t n1 = 0, n2 = 0;
     backend::longSplit(n, &n1, &n2);
-    if (ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
+    if (!work) {
+        if (ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
+        work = impl_->devWork;
+    }
     const auto& lt = impl_->twLong[n];
     const int E = backend::longE();
-    if (backend::launchLongA(dIn, impl_->devWork, n1, n2, batch, inv, impl_->twC2C[{n1, E}], lt.lo, lt.hi, s))
+    if (backend::launchLongA(dIn, work, n1, n2, batch, inv, impl_->twC2C[{n1, E}], lt.lo, lt.hi, s))
         return -5;
-    if (backend::launchLongB(impl_->devWork, dOut, n1, n2, batch, inv, scale, impl_->twC2C[{n2, E}], s))
+    if (backend::launchLongB(work, dOut, n1, n2, batch, inv, scale, impl_->twC2C[{n2, E}], s))
         return -5;
     return 0;
+}
+
+int Plan::execC2CTensor(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
+                        float scale, int splitTerms, void* stream) {
+    if (!impl_ || !dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull ||
+        (direction != -1 && direction != 1) || !backend::hasTensorVariant(n, splitTerms))
+        return -8;
+    if (prepareC2C(n, 16)) return -2;
+    if (backend::launchC2CTensor(dIn, dOut, n, batch, direction > 0, scale, impl_->twC2C[{n, 16}], splitTerms,
+                                 stream))
+        return -5;
+    return 0;
+}
+
+int Plan::tensorStatus(unsigned* status) {
+    if (!status) return -10;
+    return backend::tensorStatus(status, true) ? -6 : 0;
 }
 
 int Plan::execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
@@ -542,53 +572,86 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
     return 0;
 }
 
-// Shared body of the synchronous host-pointer entry points: upload, enqueue, sync, download.
-// enqueue() returns an exec* status: -2 prepare and -3 alloc pass through, others map to -5.
+// Body of the synchronous host-pointer entry points: upload, enqueue, synchronise, download.
+// Batches above kPipelineBytes are cut into row chunks of about kChunkBytes that rotate over
+// three streams, so the H2D of one chunk, the kernels of another and the D2H of a third
+// overlap (two copy engines).  enqueue() returns an exec status: -2 prepare and -3 alloc pass
+// through, any other failure is a launch failure (-5).
+constexpr size_t kPipelineBytes = 16u << 20, kChunkBytes = 8u << 20;
+
 template <class Enqueue>
-static int hostRoundTrip(void** dIn, size_t* inCap, void** dOut, size_t* outCap, void* stream,
-                         const float* in, size_t inBytes, float* out, size_t outBytes,
-                         Enqueue&& enqueue) {
-    if (ensureBuf(dIn, inCap, inBytes)) return -3;
-    if (ensureBuf(dOut, outCap, outBytes)) return -3;
-    if (backend::copyH2D(*dIn, in, inBytes, stream)) return -4;
-    const int lrc = enqueue(*dIn, *dOut);
-    if (lrc == -2 || lrc == -3) return lrc;
-    if (lrc) return -5;
-    if (backend::streamSync(stream)) return -6;
-    if (backend::copyD2H(out, *dOut, outBytes, stream)) return -7;
-    if (backend::streamSync(stream)) return -7;
+int Plan::roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRowBytes,
+                    uint32_t batch, Enqueue&& enqueue) {
+    Impl* im = impl_.get();
+    const size_t inBytes = inRowBytes * batch, outBytes = outRowBytes * batch;
+    if (ensureBuf(&im->devIn, &im->devInCap, inBytes)) return -3;
+    if (ensureBuf(&im->devOut, &im->devOutCap, outBytes)) return -3;
+    void* streams[3] = {stream_, nullptr, nullptr};
+    int nstreams = 1;
+    uint32_t chunk = batch;
+    if (inBytes + outBytes > kPipelineBytes) {
+        for (int i = 0; i < 2; ++i)
+            if (!im->aux[i] && backend::streamCreate(&im->aux[i])) im->aux[i] = nullptr;
+        if (im->aux[0] && im->aux[1]) {
+            streams[1] = im->aux[0];
+            streams[2] = im->aux[1];
+            nstreams = 3;
+            const size_t row = inRowBytes > outRowBytes ? inRowBytes : outRowBytes;
+            chunk = (uint32_t)std::max<size_t>(1, kChunkBytes / row);
+        }
+    }
+    int k = 0;
+    for (uint32_t r0 = 0; r0 < batch; r0 += chunk, ++k) {
+        const uint32_t rows = std::min(chunk, batch - r0);
+        void* st = streams[k % nstreams];
+        char* di = static_cast<char*>(im->devIn) + (size_t)r0 * inRowBytes;
+        char* dout = static_cast<char*>(im->devOut) + (size_t)r0 * outRowBytes;
+        if (backend::copyH2D(di, reinterpret_cast<const char*>(in) + (size_t)r0 * inRowBytes,
+                             (size_t)rows * inRowBytes, st))
+            return -4;
+        const int lrc = enqueue(di, dout, r0, rows, st);
+        if (lrc == -2 || lrc == -3) return lrc;
+        if (lrc) return -5;
+        if (nstreams == 1 && backend::streamSync(st)) return -6;
+        if (backend::copyD2H(reinterpret_cast<char*>(out) + (size_t)r0 * outRowBytes, dout,
+                             (size_t)rows * outRowBytes, st))
+            return -7;
+    }
+    for (int i = 0; i < nstreams; ++i)
+        if (backend::streamSync(streams[i])) return nstreams == 1 ? -7 : -6;
     return 0;
 }
-
-#define BFLY_ROUNDTRIP(inPtr, inBytes, outPtr, outBytes, body)                                   \
-    hostRoundTrip(&impl_->devIn, &impl_->devInCap, &impl_->devOut, &impl_->devOutCap, stream_,  \
-                  inPtr, inBytes, outPtr, outBytes, body)
 
 int Plan::run(const float* in, float* out, uint32_t n, uint32_t batch) {
     if (!in || !out || !validShape(n, batch, kRunC2C)) return -8;
     if (prepare(n, batch)) return -2;
-    const size_t bytes = (size_t)n * batch * 8;
-    return BFLY_ROUNDTRIP(in, bytes, out, bytes, [&](void* di, void* dout) {
-        return execC2C(di, dout, n, batch, -1, 1.0f, stream_);
-    });
+    return roundTrip(in, (size_t)n * 8, out, (size_t)n * 8, batch,
+                     [&](void* di, void* dout, uint32_t, uint32_t rows, void* st) {
+                         return execC2C(di, dout, n, rows, -1, 1.0f, st);
+                     });
 }
 
 int Plan::runInverse(const float* in, float* out, uint32_t n, uint32_t batch, float scale) {
     if (!in || !out || !validShape(n, batch, kRunC2C)) return -8;
     if (prepare(n, batch)) return -2;
-    const size_t bytes = (size_t)n * batch * 8;
-    return BFLY_ROUNDTRIP(in, bytes, out, bytes, [&](void* di, void* dout) {
-        return execC2C(di, dout, n, batch, 1, scale, stream_);
-    });
+    return roundTrip(in, (size_t)n * 8, out, (size_t)n * 8, batch,
+                     [&](void* di, void* dout, uint32_t, uint32_t rows, void* st) {
+                         return execC2C(di, dout, n, rows, 1, scale, st);
+                     });
 }
 
 int Plan::runLong(const float* in, float* out, uint32_t n, uint32_t batch, int direction) {
     if (!in || !out || (direction != -1 && direction != 1) || !validShape(n, batch, kRunLong)) return -8;
     if (prepare(n, batch)) return -2;
-    const size_t bytes = (size_t)n * batch * 8;
-    return BFLY_ROUNDTRIP(in, bytes, out, bytes, [&](void* di, void* dout) {
-        return execC2C(di, dout, n, batch, direction, 1.0f, stream_);
-    });
+    int e = 0, cta = 0;
+    resolve(backend::kC2C, n, &e, &cta);
+    if (!e && ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
+    // chunks on different streams use disjoint slices of the four-step workspace
+    return roundTrip(in, (size_t)n * 8, out, (size_t)n * 8, batch,
+                     [&](void* di, void* dout, uint32_t r0, uint32_t rows, void* st) {
+                         void* work = e ? nullptr : static_cast<char*>(impl_->devWork) + (size_t)r0 * n * 8;
+                         return execC2CWith(di, dout, n, rows, direction, 1.0f, st, work);
+                     });
 }
 
 int Plan::runR2C(const float* in, float* out, uint32_t n, uint32_t batch) {
@@ -596,10 +659,10 @@ int Plan::runR2C(const float* in, float* out, uint32_t n, uint32_t batch) {
     int e = 0, cta = 0;
     resolve(backend::kR2C, n, &e, &cta);
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
-    return BFLY_ROUNDTRIP(in, (size_t)n * batch * 4, out, (size_t)(n + 2) * batch * 4,
-                          [&](void* di, void* dout) {
-                             return execR2C(di, dout, n, batch, 1.0f, 1.0f, stream_);
-                         });
+    return roundTrip(in, (size_t)n * 4, out, (size_t)(n + 2) * 4, batch,
+                     [&](void* di, void* dout, uint32_t, uint32_t rows, void* st) {
+                         return execR2C(di, dout, n, rows, 1.0f, 1.0f, st);
+                     });
 }
 
 int Plan::runC2R(const float* in, float* out, uint32_t n, uint32_t batch) {
@@ -607,10 +670,10 @@ int Plan::runC2R(const float* in, float* out, uint32_t n, uint32_t batch) {
     int e = 0, cta = 0;
     resolve(backend::kC2R, n, &e, &cta);
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
-    return BFLY_ROUNDTRIP(in, (size_t)(n + 2) * batch * 4, out, (size_t)n * batch * 4,
-                          [&](void* di, void* dout) {
-                             return execC2R(di, dout, n, batch, 1.0f, 1.0f, 1.0f / (float)n, stream_);
-                         });
+    return roundTrip(in, (size_t)(n + 2) * 4, out, (size_t)n * 4, batch,
+                     [&](void* di, void* dout, uint32_t, uint32_t rows, void* st) {
+                         return execC2R(di, dout, n, rows, 1.0f, 1.0f, 1.0f / (float)n, st);
+                     });
 }
 
 int Plan::measure(uint32_t n, uint32_t batch, Metric* m) {
@@ -620,9 +683,10 @@ int Plan::measure(uint32_t n, uint32_t batch, Metric* m) {
     std::vector<float> in(nf), out(nf);
     for (size_t i = 0; i < nf; ++i) in[i] = patternAt(i);
     if (prepare(n, batch)) return -2;
-    const int first = BFLY_ROUNDTRIP(in.data(), nf * 4, out.data(), nf * 4, [&](void* di, void* dout) {
-        return execC2C(di, dout, n, batch, -1, 1.0f, stream_);
-    });
+    const int first = roundTrip(in.data(), (size_t)n * 8, out.data(), (size_t)n * 8, batch,
+                                [&](void* di, void* dout, uint32_t, uint32_t rows, void* st) {
+                                    return execC2C(di, dout, n, rows, -1, 1.0f, st);
+                                });
     if (first) return -2;
     if (!impl_->timer && backend::timerCreate(&impl_->timer)) return -3;
     // Device time per launch, best of 10 (CUDA events on the plan stream).
@@ -669,10 +733,19 @@ int Plan::measure(uint32_t n, uint32_t batch, Metric* m) {
 // ================================================================== ragged
 Ragged::~Ragged() {
     if (entries_) backend::release(entries_);
+    if (tileMap_) backend::release(tileMap_);
 }
 
 int Ragged::exec(void* stream) const {
-    return backend::launchRagged(entries_, (int)count_, total_, grid_, stream) ? -5 : 0;
+    const int r = stages_ < 0   ? backend::launchRaggedFlat(entries_, (int)count_, tileMap_, total_, stream)
+                  : stages_ > 0 ? backend::launchRaggedStaged(entries_, (int)count_, total_, grid_, stages_, stream)
+                                : backend::launchRagged(entries_, (int)count_, total_, grid_, stream);
+    return r ? -5 : 0;
+}
+
+int Ragged::deviceStatus(unsigned* status) {
+    if (!status) return -10;
+    return backend::raggedStatus(status, true) ? -6 : 0;
 }
 
 std::unique_ptr<Ragged> Plan::makeRagged(const RaggedRequest* reqs, size_t count, int* status) {
@@ -690,21 +763,31 @@ std::unique_ptr<Ragged> Plan::makeRagged(const RaggedRequest* reqs, size_t count
     uint64_t tile = 0;
     for (size_t i = 0; i < count; ++i) {
         const RaggedRequest& r = reqs[i];
-        if (prepareC2C(r.n, kRaggedE)) {
+        int logn = 0;
+        while ((1u << logn) < r.n) ++logn;
+        const int e = raggedE(logn);
+        if (prepareC2C(r.n, e)) {
             st = -2;
             return nullptr;
         }
-        int logn = 0;
-        while ((1u << logn) < r.n) ++logn;
-        const uint32_t rows = (uint32_t)kRaggedThreads / (r.n / (uint32_t)kRaggedE);
-        es[i] = RaggedEntry{r.in, r.out, impl_->twC2C[{r.n, kRaggedE}], r.batch, tile, (uint32_t)logn,
+        const uint32_t rows = raggedRows(logn);
+        es[i] = RaggedEntry{r.in, r.out, impl_->twC2C[{r.n, e}], r.batch, tile, (uint32_t)logn,
                             r.direction, r.scale, rows, 0};
         tile += (r.batch + rows - 1) / rows;
     }
     std::unique_ptr<Ragged> rg(new Ragged());
     rg->count_ = count;
     rg->total_ = tile;
-    if (backend::raggedGrid(impl_->device, &rg->grid_)) {
+    bool aligned = true;
+    for (size_t i = 0; i < count; ++i) aligned = aligned && ((uintptr_t)reqs[i].in % 16u) == 0;
+    rg->stages_ = -1;   // one tile per CTA: measured fastest on B200 (hardware CTA scheduling)
+    if (const char* env = std::getenv("BFLY_RAGGED_STAGES")) {
+        const int want = std::atoi(env);
+        if (want >= -1 && want <= 2) rg->stages_ = (aligned || want < 0) ? want : 0;
+    }
+    const int grc = rg->stages_ > 0 ? backend::raggedStagedGrid(impl_->device, rg->stages_, &rg->grid_)
+                                    : backend::raggedGrid(impl_->device, &rg->grid_);
+    if (grc) {
         st = -1;
         return nullptr;
     }
@@ -713,8 +796,30 @@ std::unique_ptr<Ragged> Plan::makeRagged(const RaggedRequest* reqs, size_t count
         st = -3;
         return nullptr;
     }
-    if (backend::copyH2D(rg->entries_, es.data(), count * sizeof(RaggedEntry), stream_) ||
-        backend::streamSync(stream_)) {
+    if (backend::copyH2D(rg->entries_, es.data(), count * sizeof(RaggedEntry), stream_)) {
+        st = -4;
+        return nullptr;
+    }
+    // request index of every tile for the one-tile-per-CTA mode (up to 4 Mi tiles = 16 MiB;
+    // larger work lists fall back to a binary search per CTA)
+    std::vector<uint32_t> map;
+    if (rg->stages_ < 0 && tile <= (4ull << 20)) {
+        map.resize(tile);
+        for (size_t i = 0; i < count; ++i) {
+            const uint64_t end = i + 1 < count ? es[i + 1].tile0 : tile;
+            for (uint64_t t = es[i].tile0; t < end; ++t) map[t] = (uint32_t)i;
+        }
+        if (backend::alloc(&rg->tileMap_, map.size() * sizeof(uint32_t))) {
+            rg->tileMap_ = nullptr;
+            st = -3;
+            return nullptr;
+        }
+        if (backend::copyH2D(rg->tileMap_, map.data(), map.size() * sizeof(uint32_t), stream_)) {
+            st = -4;
+            return nullptr;
+        }
+    }
+    if (backend::streamSync(stream_)) {
         st = -4;
         return nullptr;
     }

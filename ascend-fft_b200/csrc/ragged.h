@@ -19,10 +19,20 @@ struct RaggedEntry {
 };
 static_assert(sizeof(RaggedEntry) == 64, "RaggedEntry must stay 64 bytes");
 
-// Register radix and CTA size of the ragged kernel: every tile is 256 threads x 16 complex
-// values = 4096 points (one 4096-point row, or 4096/n rows of a shorter length).
-constexpr int kRaggedE = 16;
+#ifdef __CUDACC__
+#define BFLY_HD __host__ __device__
+#else
+#define BFLY_HD
+#endif
+
+// CTA size of the ragged kernel and the register radix per length: a tile is 256 threads x E
+// complex values (4096 points for E = 16: one 4096-point row, or 4096/n rows of a shorter
+// length; 2048 points for the short lengths that run faster with E = 8).
 constexpr int kRaggedThreads = 256;
 constexpr uint32_t kRaggedMinN = 32, kRaggedMaxN = 4096;
+BFLY_HD constexpr int raggedE(int logn) { return logn <= 6 ? 8 : 16; }
+BFLY_HD constexpr uint32_t raggedRows(int logn) {
+    return (uint32_t)kRaggedThreads / ((1u << logn) / (uint32_t)raggedE(logn));
+}
 
 }  // namespace bfly

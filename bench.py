@@ -3,15 +3,17 @@
 Workload (the configuration the headline metric is quoted on): plain fp32 C2C forward over
 the 49-point grid N in {64..4096} x batch in {1..4096}, interleaved complex, Re/Im i.i.d.
 N(0,1) seeded per point (seed = 1000*log2 N + log2 batch + 1).  One step = one forward
-transform of every grid point (49 kernel launches, captured in a CUDA graph) on inputs resident
-in HBM.  The step touches 355 MB of input and 355 MB of output, more than the 126 MB L2, so
-no explicit flush is needed between steps.
+transform of every grid point on inputs resident in HBM, run as ONE ragged launch
+(k_ragged_flat over the 49 requests: 10,931 tiles of 4096 or 2048 points, one per CTA).  The step touches 355 MB of input and 355 MB of output, more
+than the 126 MB L2, so no explicit flush is needed between steps.  The same step as 49
+per-point launches replayed from a CUDA graph is reported beside it (per_point_graph).
 
   value      algorithmic bytes (16 * N * batch summed over the grid) / device time per step
   e2e        the same metric through the C ABI's synchronous host-pointer entry point
              (bfly_plan_run_c2c) with pinned host buffers: H2D + kernel + D2H timed per step
-  roofline   the dominant launch (N=4096, batch=4096) timed alone with CUDA events on its
-             stream against the measured HBM copy bandwidth
+  roofline   the step's only kernel (k_ragged_flat over the grid) timed with CUDA events on its
+             stream against the measured HBM copy bandwidth; the largest single-size launch
+             (N=4096, batch=4096, k_c2c) is reported beside it (largest_launch)
   cpu_baseline  the reference's own CPU FFT (its FP64 oracle src/framework/reference.cpp,
              compiled from its sources into oracle/_ref) on a bounded sample of the grid,
              rows spread over the host's threads
@@ -65,73 +67,103 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def dominant_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, or None."""
+def dominant_traffic(key="ragged_grid49"):
+    """DRAM bytes per launch of the step's kernel from the committed ncu summary, or None."""
     p = ROOT / "profiles" / "roofline_traffic.txt"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
         parts = line.split()
-        if len(parts) == 2 and parts[0] == "c2c_fwd_n4096_b4096":
+        if len(parts) == 2 and parts[0] == key:
             return int(parts[1])
     return None
 
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled every ~1 ms through NVML in a background thread
+    while the timed region runs (nvidia-smi -lms 100 as a fallback)."""
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, index: int, bus_id: str | None = None):
+        self.index, self.bus_id = index, bus_id
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._thread = None
+        self._proc = None
+
+    def _nvml_loop(self, nv, h):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.001)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            if self.bus_id:
+                try:
+                    h = nv.nvmlDeviceGetHandleByPciBusId(self.bus_id.encode())
+                except Exception:
+                    h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self._thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self._thread.start()
         except Exception:
-            self.proc = None
+            try:
+                self._proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,"
+                     "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                     "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                     "--format=csv,noheader,nounits", "-lms", "100"],
+                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self._thread = threading.Thread(target=self._smi_loop, daemon=True)
+                self._thread.start()
+            except Exception:
+                self._proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _smi_loop(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self._proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            try:
+                self.samples.append(float(parts[0]))
+                self.max_mhz = float(parts[1])
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, parts[2:6]):
+                if val.lower().startswith("active"):
+                    self.reasons.add(name)
 
     def __exit__(self, *exc):
-        if self.proc:
+        self._stop.set()
+        if self._proc:
             time.sleep(0.15)
-            self.proc.terminate()
+            self._proc.terminate()
             try:
-                self.proc.wait(timeout=5)
+                self._proc.wait(timeout=5)
             except Exception:
-                self.proc.kill()
+                self._proc.kill()
+        if self._thread:
+            self._thread.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 8:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[4:8]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
 # ------------------------------------------------------------------ CPU reference
@@ -256,6 +288,7 @@ def run_ours(args):
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
     import bfly
+    import oracle.fft_oracle as O
 
     ctx = bfly.Context()
     rc = ctx.init(device=dev.index)
@@ -275,76 +308,92 @@ def run_ours(args):
     for n, b, x, y in pts:   # builds twiddle tables outside any capture
         assert plan.prepare(n, b) == 0
 
-    def step():
+    def check(tag):
+        worst = 0.0
+        for n, b, x, y in pts:
+            rows = O.sample_batches(b, 2)
+            ref = np.fft.fft(x[rows].cpu().numpy().astype(np.complex128), axis=-1)
+            worst = max(worst, O.rel_l2_rows(y[rows].cpu().numpy(), ref))
+        assert worst <= 1e-6, f"{tag} parity check failed: rel L2 {worst}"
+        return worst
+
+    def per_point():
         for n, b, x, y in pts:
             r = plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh)
             if r:
                 raise RuntimeError(f"exec_c2c({n},{b}) = {r}")
 
-    # parity spot check of the product path before timing
+    # the product path: one ragged persistent launch over all 49 requests
+    ragged = plan.make_ragged((x.data_ptr(), y.data_ptr(), n, b, -1, 1.0) for n, b, x, y in pts)
+
+    def ragged_step():
+        r = ragged.exec(sh)
+        if r:
+            raise RuntimeError(f"ragged exec = {r}")
+
+    # parity spot checks of both paths before timing
     with torch.cuda.stream(stream):
-        step()
+        per_point()
     stream.synchronize()
-    import oracle.fft_oracle as O
-    worst = 0.0
-    for n, b, x, y in pts:
-        rows = O.sample_batches(b, 2)
-        ref = np.fft.fft(x[rows].cpu().numpy().astype(np.complex128), axis=-1)
-        worst = max(worst, O.rel_l2_rows(y[rows].cpu().numpy(), ref))
-    assert worst <= 1e-6, f"parity check failed: rel L2 {worst}"
-
-    graph = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(graph, stream=stream):
-        step()
-    launches_per_step = len(pts)
-
-    def replay():
-        with torch.cuda.stream(stream):
-            graph.replay()
-
-    for _ in range(max(3, args.warmup)):
-        replay()
-    stream.synchronize()
-    if dist:
-        dist.barrier()
+    worst = check("per-point")
+    for _, _, _, y in pts:
+        y.zero_()
     torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev.index) as clocks:
+    ragged_step()
+    stream.synchronize()
+    worst = max(worst, check("ragged"))
+
+    def timed(fn, steps, sample_clocks=False):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        bus = getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None)
+        sampler = ClockSampler(dev.index, bus) if sample_clocks else None
+        if sampler:
+            sampler.__enter__()
         e0.record(stream)
-        for _ in range(args.steps):
-            replay()
+        for _ in range(steps):
+            fn()
         e1.record(stream)
         e1.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    torch.cuda.synchronize()
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
-        dist.barrier()
+        if sampler:
+            sampler.__exit__(None, None, None)
+        t = e0.elapsed_time(e1) / steps
+        torch.cuda.synchronize()
+        if dist:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = tt.item()
+        return t, sampler
+
+    ms, clocks = timed(ragged_step, args.steps, sample_clocks=True)
     total_bytes = grid_bytes() * world
     value = total_bytes / (ms / 1e3) / 1e9
 
-    # roofline: the dominant launch timed alone on its stream
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        per_point()
+
+    def graph_step():
+        with torch.cuda.stream(stream):
+            graph.replay()
+
+    ms_graph, _ = timed(graph_step, args.steps)
+    per_point_gbs = total_bytes / (ms_graph / 1e3) / 1e9
+
+    # the largest single-size launch timed alone on its stream
     n, b = DOMINANT
     xd = next(x for (nn, bb, x, y) in pts if (nn, bb) == DOMINANT)
     yd = torch.empty_like(xd)
-    reps = 50
-    for _ in range(5):
-        plan.exec_c2c(xd.data_ptr(), yd.data_ptr(), n, b, -1, 1.0, sh)
-    stream.synchronize()
-    d0 = torch.cuda.Event(enable_timing=True)
-    d1 = torch.cuda.Event(enable_timing=True)
-    d0.record(stream)
-    for _ in range(reps):
-        plan.exec_c2c(xd.data_ptr(), yd.data_ptr(), n, b, -1, 1.0, sh)
-    d1.record(stream)
-    d1.synchronize()
-    dom_ms = d0.elapsed_time(d1) / reps
+    dom_ms, _ = timed(lambda: plan.exec_c2c(xd.data_ptr(), yd.data_ptr(), n, b, -1, 1.0, sh), 50)
     dom_bytes = 16 * n * b
     peak, peak_kind = load_peaks()
-    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    achieved = grid_bytes() / (ms / 1e3) / 1e9
 
     # e2e through the C ABI with pinned host buffers: H2D + kernel + D2H per grid point
     host = []
@@ -356,6 +405,8 @@ def run_ours(args):
     for nn, bb, hx, hy in host:   # warm-up (device buffers grow to the largest point)
         assert plan.run(hx, hy, nn, bb) == 0
     e2e_steps = max(1, min(args.steps, 5))
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         for nn, bb, hx, hy in host:
@@ -369,6 +420,9 @@ def run_ours(args):
         e2e_s = t.item()
     h2d = sum(8 * nn * bb for nn, bb, _, _ in host)
     e2e_value = grid_bytes() * world / e2e_s / 1e9
+    info = ragged.info()
+    ragged.close()
+    del graph
 
     if dist:
         dist.barrier()
@@ -387,21 +441,27 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "points": len(pts), "bytes_per_step": grid_bytes() * world,
+        "config": {"workload": WORKLOAD, "points": len(pts), "bytes_per_step": total_bytes,
                    "l2": "355 MB in + 355 MB out per step > 126 MB L2; no flush",
-                   "launch": "49 launches per step replayed from one CUDA graph",
+                   "launch": "one ragged launch (k_ragged_flat, one tile per CTA) per step",
                    "parallelism": f"batch-sharded replicas x{world}", "candidate": plan.candidate_id,
-                   "parity_rel_l2_max": worst},
+                   "ragged": info, "parity_rel_l2_max": worst},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": dominant_traffic(),
-                     "kernel": "k_c2c<4096,16,1,fwd> N=4096 batch=4096", "peak_kind": peak_kind,
-                     "launch_us": round(dom_ms * 1e3, 3), "algorithmic_bytes": dom_bytes},
+                     "kernel": "k_ragged_flat over the 49-point grid", "peak_kind": peak_kind,
+                     "launch_us": round(ms * 1e3, 3), "algorithmic_bytes": grid_bytes()},
+        "per_point_graph": {"value": round(per_point_gbs, 2), "unit": UNIT,
+                            "ms_per_step": round(ms_graph, 5), "launches_per_step": len(pts)},
+        "largest_launch": {"kernel": "k_c2c<4096,16,1,fwd> N=4096 batch=4096",
+                           "achieved": round(dom_bytes / (dom_ms / 1e3) / 1e9, 2),
+                           "frac": round(dom_bytes / (dom_ms / 1e3) / 1e9 / peak, 4),
+                           "launch_us": round(dom_ms * 1e3, 3)},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": h2d, "path": "bfly_plan_run_c2c, pinned host buffers"},
-        "gpu_launches": launches_per_step * args.steps,
-        "clocks": clocks.summary(),
+                "d2h_bytes_per_step": h2d,
+                "path": "bfly_plan_run_c2c per grid point, pinned host buffers, copies pipelined"},
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary() if clocks else None,
         "cpu_baseline": cpu,
-        "frac_of_roofline_step": round(value / world / peak, 4),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -413,11 +473,27 @@ def run_case(spec: str, reps: int):
     import torch
     import bfly
     kind, n, b = spec.split(":")
-    n, b = int(n), int(b)
     dev = torch.device("cuda", 0)
     ctx = bfly.Context()
     assert ctx.init() == 0
     plan = ctx.make_plan()
+    if kind == "ragged":   # ragged:grid:CAP -> the 49-point grid with batch capped at CAP
+        cap = int(b)
+        bufs = []
+        for nn in GRID_N:
+            for bb in GRID_B:
+                bb = min(bb, cap)
+                x = torch.randn(bb, nn, dtype=torch.complex64, device=dev)
+                bufs.append((x, torch.empty_like(x), nn, bb))
+        rg = plan.make_ragged((x.data_ptr(), y.data_ptr(), nn, bb, -1, 1.0) for x, y, nn, bb in bufs)
+        for _ in range(reps):
+            r = rg.exec(0)
+            if r:
+                raise SystemExit(f"{spec}: status {r}")
+        torch.cuda.synchronize()
+        print(f"case {spec} x{reps} ok, {sum(16 * nn * bb for _, _, nn, bb in bufs)} bytes per launch")
+        return 0
+    n, b = int(n), int(b)
     g = torch.Generator(device=dev).manual_seed(grid_seed(n, b))
     if kind in ("c2c", "c2c_inv"):
         x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)

@@ -143,14 +143,22 @@ public:
     uint64_t tiles() const { return total_; }
     int grid() const { return grid_; }
     size_t requests() const { return count_; }
+    // Launch mode: -1 (default) one tile per CTA, scheduled by the hardware; 0 persistent CTAs
+    // with plain loads; 1 or 2 persistent CTAs with tiles staged in shared memory by bulk copies
+    // (all inputs 16-byte aligned).  The environment variable BFLY_RAGGED_STAGES overrides.
+    int stages() const { return stages_; }
+    // Device status of staged launches: 0, or 1 when a bounded wait ran out (then cleared).
+    static int deviceStatus(unsigned* status);
 
 private:
     friend class Plan;
     Ragged() = default;
     void* entries_ = nullptr;
+    void* tileMap_ = nullptr;   // request index per tile (one-tile-per-CTA mode)
     size_t count_ = 0;
     uint64_t total_ = 0;
     int grid_ = 0;
+    int stages_ = 0;
 };
 
 class Plan {
@@ -191,6 +199,14 @@ public:
     int execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
                 float sInt, float outScale, void* stream);
 
+    // Split-BF16 tensor-core C2C (5th-generation tensor cores, fp32 accumulate): every radix-16
+    // pass is a dense contraction with the DFT-16 matrix, operands split into `splitTerms` = 2
+    // (hi+lo, 3 products) or 3 (hi+mid+lo, 6 products) bf16 terms.  n in {256, 4096}.
+    int execC2CTensor(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
+                      float scale, int splitTerms, void* stream);
+    // Device status of the tensor-core launches: 0, or 1 when a bounded MMA wait ran out.
+    static int tensorStatus(unsigned* status);
+
     // Build a ragged persistent launch over `count` requests; *status receives 0 or a code
     // (-8 invalid request, -2 table build, -3 alloc, -4 upload, -1 runtime).
     std::unique_ptr<Ragged> makeRagged(const RaggedRequest* reqs, size_t count, int* status);
@@ -206,6 +222,13 @@ private:
     int prepareReal(uint32_t n);
     int prepareLong(uint32_t n);
     int resolve(int kind, uint32_t n, int* e, int* cta) const;
+    int execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
+                    float scale, void* stream, void* work);
+    // Upload / enqueue / download of host buffers, pipelined over row chunks on several
+    // streams for large batches.  enqueue(dIn, dOut, firstRow, rows, stream) -> exec status.
+    template <class Enqueue>
+    int roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRowBytes,
+                  uint32_t batch, Enqueue&& enqueue);
     Candidate cand_;
     std::vector<Transform> tf_;
     std::unique_ptr<Impl> impl_;

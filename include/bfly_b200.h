@@ -124,6 +124,19 @@ int bfly_plan_exec_c2r_async(bfly_plan* plan, const void* d_in, void* d_out, uin
                              uint64_t batch, float s_edge, float s_int, float out_scale,
                              void* stream);
 
+/* New: split-BF16 tensor-core C2C on the 5th-generation tensor cores (tcgen05, fp32
+ * accumulate in tensor memory): each radix-16 pass is a dense contraction with the DFT-16
+ * matrix; operands split into split_terms = 2 (hi+lo, 3 products) or 3 (hi+mid+lo, 6 products)
+ * bf16 terms.  n in {256, 4096}; direction -1 / +1; output times scale; asynchronous on
+ * `stream`.  The reference has no counterpart (its Cube-unit probe src/ascendc/cube_probe.cpp
+ * never reached a usable matrix unit). */
+int bfly_plan_exec_c2c_tc_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
+                                uint64_t batch, int direction, float scale, int split_terms,
+                                void* stream);
+/* Status word of the tensor-core launches on the current device: 0, or 1 when a bounded wait
+ * for an MMA ran out (the launch then stopped early); reading clears it. */
+int bfly_tc_device_status(unsigned* status);
+
 /* New: ragged persistent launch.  One kernel launch transforms a set of requests with
  * different lengths (32..4096, powers of two), batch counts and directions; the work list is
  * built once on the device and exec is a single launch that can be captured in a CUDA graph.
@@ -143,7 +156,13 @@ typedef struct bfly_ragged_request {
 int bfly_ragged_create(bfly_plan* plan, const bfly_ragged_request* reqs, size_t count,
                        bfly_ragged** out);
 int bfly_ragged_exec_async(bfly_ragged* ragged, void* stream);
-int bfly_ragged_info(bfly_ragged* ragged, uint64_t* tiles, int* grid);
+/* tiles, resident grid and launch mode: -1 (default) one 4096-point tile per CTA, scheduled by
+ * the hardware; 0 persistent CTAs with plain loads; 1, 2 persistent CTAs with bulk-copy staged
+ * tiles (every input 16-byte aligned).  BFLY_RAGGED_STAGES=-1/0/1/2 overrides. */
+int bfly_ragged_info(bfly_ragged* ragged, uint64_t* tiles, int* grid, int* stages);
+/* Status word of the staged launches on the current device: 0, or 1 when a bounded wait for a
+ * staged copy ran out (the launch then stopped early); reading clears it. */
+int bfly_ragged_device_status(unsigned* status);
 void bfly_ragged_destroy(bfly_ragged* ragged);
 
 /* New: long C2C (four-step, n in {8192, 16384, 32768, 65536}) that allocates no device memory,

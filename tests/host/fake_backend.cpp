@@ -155,5 +155,21 @@ int launchRagged(const void* entries, int count, uint64_t, int, void*) {
     return 0;
 }
 
+int raggedStagedGrid(int, int stages, int* grid) { *grid = 148 * (stages == 1 ? 3 : 2); return 0; }
+int launchRaggedStaged(const void* entries, int count, uint64_t tiles, int grid, int, void* s) {
+    return launchRagged(entries, count, tiles, grid, s);
+}
+int raggedStatus(unsigned* status, bool) { *status = 0; return 0; }
+int launchRaggedFlat(const void* entries, int count, const void*, uint64_t tiles, void* s) {
+    return launchRagged(entries, count, tiles, 0, s);
+}
+
+bool hasTensorVariant(uint32_t n, int split) { return (n == 256 || n == 4096) && (split == 2 || split == 3); }
+int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+                    const void* tw, int, void* s) {
+    return launchC2C(in, out, n, batch, inverse, scale, tw, 16, 256, s);
+}
+int tensorStatus(unsigned* status, bool) { *status = 0; return 0; }
+
 }  // namespace backend
 }  // namespace bfly

@@ -270,6 +270,26 @@ int main(int argc, char** argv) {
     CHECK(plan->runInverse(out.data(), out.data(), n, batch, 1.0f / n) == 0);
     for (size_t i = 0; i < in.size(); ++i) CHECK(std::fabs(out[i] - in[i]) < 1e-5);
 
+    // ---- large batch: the round trip is pipelined over row chunks on three streams
+    {
+        const uint32_t bn = 64, bb = 17000;   // 2 x 8.7 MB > 16 MB pipelining threshold
+        std::vector<float> bin(2 * (size_t)bn * bb), bout(bin.size()), bref(2 * bn);
+        for (size_t i = 0; i < bin.size(); ++i) bin[i] = bfly::patternAt(i * 3 + 1);
+        const int streamsBefore = fake::streamsCreated;
+        CHECK(plan->run(bin.data(), bout.data(), bn, bb) == 0);
+        CHECK(fake::streamsCreated == streamsBefore + 2);
+        uint32_t rows[8];
+        const uint32_t cnt = bfly::sampleBatches(bb, 8, rows, 8);
+        for (uint32_t i = 0; i < cnt; ++i) {
+            bfly::refFftF32(bin.data() + (size_t)rows[i] * 2 * bn, bref.data(), bn);
+            CHECK(bfly::maxRelScaled(bout.data() + (size_t)rows[i] * 2 * bn, bref.data(), 2 * bn) < 1e-5);
+        }
+        fake::failCopy = fake::copies + 3;   // the second chunk's upload
+        const int rc = plan->run(bin.data(), bout.data(), bn, bb);
+        CHECK(rc == -4);
+        fake::failCopy = 0;
+    }
+
     // ---- measure: acceptance against the FP64 check, state transitions
     CHECK(plan->measure(64, 2, &metric) == 0);
     CHECK(metric.measuredOk && metric.maxRelErr < 1e-5 && plan->candidate().state == bfly::State::Measured);
@@ -312,7 +332,7 @@ int main(int argc, char** argv) {
         bfly::RaggedRequest ok[] = {{a.data(), oa.data(), 64, 3, -1, 1.f}, {b.data(), ob.data(), 128, 2, 1, 0.5f}};
         auto rg = plan->makeRagged(ok, 2, &st);
         CHECK(rg && st == 0 && rg->requests() == 2);
-        CHECK(rg->tiles() == 1 + 1);   // 64-point: 64 rows per tile; 128-point: 32 rows per tile
+        CHECK(rg->tiles() == 1 + 1);   // 64-point: 32 rows per tile; 128-point: 32 rows per tile
         CHECK(rg->exec(nullptr) == 0);
         for (uint32_t row = 0; row < 3; ++row) {
             bfly::refFftF32(a.data() + row * 128, r.data(), 64);

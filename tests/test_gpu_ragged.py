@@ -34,16 +34,43 @@ def _check(bufs, tol=1e-6):
     return worst
 
 
-def test_ragged_config_mix(ctx, cuda):
+@pytest.mark.parametrize("stages", ["-1", "0", "1", "2"])
+def test_ragged_config_mix(ctx, cuda, stages, monkeypatch):
+    """The 256-request mix: one tile per CTA (-1), persistent CTAs with plain loads (0) and with
+    bulk-copy staged tiles (1, 2)."""
     import torch
+    monkeypatch.setenv("BFLY_RAGGED_STAGES", stages)
     reqs = O.ragged_requests(256, 7)
     plan, ragged, bufs = _build(ctx, cuda, reqs)
     info = ragged.info()
-    assert info["tiles"] > 0 and info["grid"] > 0
+    assert info["tiles"] > 0 and info["grid"] > 0 and info["stages"] == int(stages)
     assert ragged.exec(torch.cuda.current_stream().cuda_stream) == 0
     torch.cuda.synchronize()
+    assert ragged.device_status() == 0
     _check(bufs)
     ragged.close()
+
+
+def test_ragged_unaligned_inputs_use_plain_loads(ctx, cuda):
+    """An input that is only 8-byte aligned cannot be bulk-copied: asking for staged tiles
+    falls back to the plain persistent kernel."""
+    import torch
+    plan = ctx.make_plan()
+    n, b = 256, 33
+    base = torch.randn(b * n + 1, dtype=torch.complex64, device=cuda)
+    x = base[1:].view(b, n)                      # 8-byte offset
+    y = torch.empty(b, n, dtype=torch.complex64, device=cuda)
+    os = __import__("os")
+    os.environ["BFLY_RAGGED_STAGES"] = "1"
+    try:
+        rg = plan.make_ragged([(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0)])
+    finally:
+        del os.environ["BFLY_RAGGED_STAGES"]
+    assert x.data_ptr() % 16 == 8 and rg.info()["stages"] == 0
+    assert rg.exec(0) == 0
+    torch.cuda.synchronize()
+    ref = np.fft.fft(x.cpu().numpy().astype(np.complex128), axis=-1)
+    assert O.rel_l2_rows(y.cpu().numpy(), ref) <= 1e-6
 
 
 def test_ragged_every_length_and_partial_tiles(ctx, cuda):
