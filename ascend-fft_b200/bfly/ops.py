@@ -23,11 +23,23 @@ import torch
 from .core import DEFAULT_CANDIDATE, BflyError, Context
 
 _lock = threading.Lock()
-_state = {}   # device index -> (Context, Plan)
+_state = {}   # device index -> {"ctx": Context, "plans": {candidate id: Plan}, "tuned": {...}}
+
+# Kernel variant per length measured fastest on B200 (radix = complex values per thread,
+# cta = threads per CTA); lengths not listed use DEFAULT_CANDIDATE.  C2C keys are the transform
+# length, real-transform keys the inner complex length n/2.
+BEST_C2C = {32: "r8_cta256_shared_fp32_stockham", 64: "r8_cta256_shared_fp32_stockham",
+            128: "r16_cta128_shared_fp32_stockham", 256: "r16_cta128_shared_fp32_stockham",
+            512: "r16_cta128_shared_fp32_stockham", 1024: "r16_cta256_shared_fp32_stockham",
+            2048: "r16_cta128_shared_fp32_stockham", 4096: "r16_cta256_shared_fp32_stockham",
+            8192: "r16_cta512_shared_fp32_stockham"}
+BEST_REAL = {32: "r8_cta256_shared_fp32_stockham", 64: "r8_cta256_shared_fp32_stockham",
+             128: "r16_cta128_shared_fp32_stockham", 256: "r16_cta128_shared_fp32_stockham",
+             512: "r16_cta128_shared_fp32_stockham", 1024: "r16_cta128_shared_fp32_stockham",
+             2048: "r16_cta128_shared_fp32_stockham"}
 
 
-def plan_for(device: torch.device):
-    """Per-device context and default plan (created on first use)."""
+def _device_state(device: torch.device):
     idx = device.index if device.index is not None else torch.cuda.current_device()
     with _lock:
         if idx not in _state:
@@ -35,11 +47,49 @@ def plan_for(device: torch.device):
             rc = ctx.init(device=idx)
             if rc != 0:
                 raise BflyError("Context.init", rc)
-            plan = ctx.make_plan(DEFAULT_CANDIDATE)
-            if plan is None:
-                raise BflyError("make_plan", -1)
-            _state[idx] = (ctx, plan)
-        return _state[idx][1]
+            _state[idx] = {"ctx": ctx, "plans": {}, "tuned": {}}
+        return _state[idx]
+
+
+def _plan_by_id(st, cid: str, n: int):
+    with _lock:
+        p = st["plans"].get(cid)
+        if p is None:
+            p = st["ctx"].make_plan(cid, n, 1)
+            if p is None:
+                raise BflyError(f"make_plan({cid})", -1)
+            st["plans"][cid] = p
+        return p
+
+
+def plan_for(device: torch.device, n: int | None = None, kind: str = "c2c"):
+    """Plan serving a transform of length n on `device`: an autotuned choice when one was made
+    with autotune(), else the measured per-length default, else DEFAULT_CANDIDATE."""
+    st = _device_state(device)
+    if n is not None and (kind, n) in st["tuned"]:
+        return st["tuned"][(kind, n)]
+    table = BEST_C2C if kind == "c2c" else BEST_REAL
+    key = n if kind == "c2c" else (n // 2 if n else None)
+    cid = table.get(key, DEFAULT_CANDIDATE) if key is not None else DEFAULT_CANDIDATE
+    return _plan_by_id(st, cid, 1024)   # every tabled candidate is feasible at 1024
+
+
+def autotune(n: int, batch: int, device: torch.device | None = None, top_k: int = 3,
+             cache: str | None = None):
+    """Measure candidates for a C2C of length n with the library's autotuner (Context.select)
+    and use the fastest for later fft/ifft calls of that length; the choice is persisted in the
+    JSON tuning cache `cache` (default $BFLY_TUNING_CACHE, else none).  Returns the log."""
+    import os
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    st = _device_state(device)
+    path = cache or os.environ.get("BFLY_TUNING_CACHE")
+    if path:
+        st["ctx"].set_tuning_cache(path)
+    plan, log = st["ctx"].select(n, batch, top_k, want_log=True)
+    if plan is None:
+        raise BflyError(f"select(n={n}, batch={batch})", -1)
+    st["tuned"][("c2c", n)] = plan
+    return log
 
 
 def _stream(t: torch.Tensor) -> int:
@@ -72,7 +122,7 @@ def c2c(x: torch.Tensor, direction: int, scale: float, out: torch.Tensor | None 
     y = out if out is not None else torch.empty_like(x)
     if batch == 0:
         return y
-    rc = plan_for(x.device).exec_c2c(x.data_ptr(), y.data_ptr(), n, batch, direction, scale, _stream(x))
+    rc = plan_for(x.device, n).exec_c2c(x.data_ptr(), y.data_ptr(), n, batch, direction, scale, _stream(x))
     if rc:
         raise BflyError(f"exec_c2c(n={n}, batch={batch})", rc)
     return y
@@ -86,7 +136,7 @@ def r2c(x: torch.Tensor, s_edge: float = 1.0, s_int: float = 1.0) -> torch.Tenso
     y = torch.empty(*x.shape[:-1], n // 2 + 1, dtype=torch.complex64, device=x.device)
     if batch == 0:
         return y
-    rc = plan_for(x.device).exec_r2c(x.data_ptr(), y.data_ptr(), n, batch, s_edge, s_int, _stream(x))
+    rc = plan_for(x.device, n, "real").exec_r2c(x.data_ptr(), y.data_ptr(), n, batch, s_edge, s_int, _stream(x))
     if rc:
         raise BflyError(f"exec_r2c(n={n}, batch={batch})", rc)
     return y
@@ -104,8 +154,8 @@ def c2r(X: torch.Tensor, n: int, s_edge: float = 1.0, s_int: float = 1.0,
         return y
     if out_scale is None:
         out_scale = 1.0 / n
-    rc = plan_for(X.device).exec_c2r(X.data_ptr(), y.data_ptr(), n, batch, s_edge, s_int, out_scale,
-                                     _stream(X))
+    rc = plan_for(X.device, n, "real").exec_c2r(X.data_ptr(), y.data_ptr(), n, batch, s_edge, s_int,
+                                                out_scale, _stream(X))
     if rc:
         raise BflyError(f"exec_c2r(n={n}, batch={batch})", rc)
     return y
@@ -126,8 +176,7 @@ class _RFFT(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, scale):
         ctx.scale, ctx.n = scale, x.shape[-1]
-        y = r2c(x)
-        return y if scale == 1.0 else y * scale
+        return r2c(x, scale, scale)   # the scale rides on the kernel's per-bin weights
 
     @staticmethod
     def backward(ctx, g):
@@ -144,6 +193,22 @@ class _IRFFT(torch.autograd.Function):
     def backward(ctx, g):
         c = ctx.scale
         return r2c(g.contiguous(), c, 2.0 * c), None, None
+
+
+def c2c_tensor(x: torch.Tensor, direction: int = -1, scale: float = 1.0, split_terms: int = 3) -> torch.Tensor:
+    """Split-BF16 tensor-core C2C (n = 256 or 4096) on torch's current stream."""
+    _need_cuda(x, torch.complex64, "c2c_tensor")
+    x = x.contiguous()
+    n = x.shape[-1]
+    batch = x.numel() // n if n else 0
+    y = torch.empty_like(x)
+    if batch == 0:
+        return y
+    rc = plan_for(x.device, n).exec_c2c_tc(x.data_ptr(), y.data_ptr(), n, batch, direction, scale,
+                                           split_terms, _stream(x))
+    if rc:
+        raise BflyError(f"exec_c2c_tc(n={n}, batch={batch})", rc)
+    return y
 
 
 def fft(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:

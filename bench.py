@@ -67,16 +67,21 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def dominant_traffic(key="ragged_grid49"):
-    """DRAM bytes per launch of the step's kernel from the committed ncu summary, or None."""
+def dominant_traffic():
+    """DRAM bytes of one full-grid launch of the step's kernel: the committed ncu capture of the
+    capped grid (profiles/roofline_traffic.txt) scaled by algorithmic bytes, or None."""
     p = ROOT / "profiles" / "roofline_traffic.txt"
     if not p.exists():
         return None
+    vals = {}
     for line in p.read_text().splitlines():
         parts = line.split()
-        if len(parts) == 2 and parts[0] == key:
-            return int(parts[1])
-    return None
+        if len(parts) == 2 and not parts[0].startswith("#"):
+            vals[parts[0]] = int(parts[1])
+    t, a = vals.get("ragged_grid49_cap1024"), vals.get("ragged_grid49_cap1024_algorithmic")
+    if not t or not a:
+        return None
+    return int(round(t * grid_bytes() / a))
 
 
 # ------------------------------------------------------------------ clocks
@@ -276,6 +281,93 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ our arm
+def extra_measurements(dev, stream):
+    """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores vs fp32 at the
+    largest power-of-16 grid points; long C2C forward + backward (four-step, batch*n = 2^26);
+    real transforms forward + adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
+    events on `stream` (20 launches after 3 warm-ups) and the error against FP64 on sampled rows."""
+    import torch
+    import bfly
+    import oracle.fft_oracle as O
+    sh = stream.cuda_stream
+    peak, _ = load_peaks()
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def rel(y, x, inverse=False, rows=4):
+        idx = O.sample_batches(x.shape[0], rows)
+        xs = x[idx].cpu().numpy().astype(np.complex128)
+        ref = np.fft.ifft(xs, axis=-1) * xs.shape[-1] if inverse else np.fft.fft(xs, axis=-1)
+        return O.rel_l2_rows(y[idx].cpu().numpy(), ref)
+
+    out = {"split_bf16": {}, "long_fwd_bwd": {}, "real_fwd_adjoint": {}}
+    # ---- split-BF16 tensor cores vs plain fp32
+    for n, b in ((4096, 4096), (256, 4096)):
+        g = torch.Generator(device=dev).manual_seed(grid_seed(n, b))
+        x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.empty_like(x)
+        byts = 16 * n * b
+        plan = bfly.plan_for(dev, n)
+        res = {}
+        for tag, fn in (("fp32", lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh)),
+                        ("tc_split3", lambda: plan.exec_c2c_tc(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, 3, sh)),
+                        ("tc_split2", lambda: plan.exec_c2c_tc(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, 2, sh))):
+            ms = timed(fn)
+            gbs = byts / (ms / 1e3) / 1e9
+            res[tag] = {"gbs": round(gbs, 1), "frac": round(gbs / peak, 4), "rel_l2": rel(y, x)}
+        res["speedup_split3_vs_fp32"] = round(res["tc_split3"]["gbs"] / res["fp32"]["gbs"], 3)
+        res["speedup_split2_vs_fp32"] = round(res["tc_split2"]["gbs"] / res["fp32"]["gbs"], 3)
+        out["split_bf16"][f"n{n}_b{b}"] = res
+        del x, y
+    # ---- long C2C forward + backward (the backward is the conjugate-FFT adjoint)
+    for n in (8192, 16384, 32768, 65536):
+        b = (1 << 26) // n
+        g = torch.Generator(device=dev).manual_seed(11)
+        x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.empty_like(x)
+        z = torch.empty_like(x)
+        plan = bfly.plan_for(dev, n)
+        byts = 16 * n * b
+        ms_f = timed(lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh))
+        ms_b = timed(lambda: plan.exec_c2c(y.data_ptr(), z.data_ptr(), n, b, 1, 1.0, sh))
+        out["long_fwd_bwd"][f"n{n}_b{b}"] = {
+            "fwd_gbs": round(byts / (ms_f / 1e3) / 1e9, 1), "bwd_gbs": round(byts / (ms_b / 1e3) / 1e9, 1),
+            "fwd_bwd_gbs": round(2 * byts / ((ms_f + ms_b) / 1e3) / 1e9, 1),
+            "fwd_rel_l2": rel(y, x, rows=2), "bwd_rel_l2": rel(z, y, inverse=True, rows=2),
+            "schedule": "single pass" if n <= 8192 else "four-step (2 HBM passes)"}
+        del x, y, z
+    # ---- real transforms: R2C forward and its adjoint (weighted C2R), batch 1024
+    for n in (128, 1024, 4096, 8192):
+        b = 1024
+        g = torch.Generator(device=dev).manual_seed(n)
+        x = torch.rand(b, n, device=dev, generator=g) * 2 - 1
+        X = torch.empty(b, n // 2 + 1, dtype=torch.complex64, device=dev)
+        gx = torch.empty_like(x)
+        plan = bfly.plan_for(dev, n, "real")
+        byts = (8 * n + 8) * b
+        ms_f = timed(lambda: plan.exec_r2c(x.data_ptr(), X.data_ptr(), n, b, 1.0, 1.0, sh))
+        ms_b = timed(lambda: plan.exec_c2r(X.data_ptr(), gx.data_ptr(), n, b, 1.0, 0.5, 1.0, sh))
+        idx = O.sample_batches(b, 4)
+        ref = np.fft.rfft(x[idx].cpu().numpy().astype(np.float64), axis=-1)
+        out["real_fwd_adjoint"][f"n{n}_b{b}"] = {
+            "r2c_gbs": round(byts / (ms_f / 1e3) / 1e9, 1), "adjoint_c2r_gbs": round(byts / (ms_b / 1e3) / 1e9, 1),
+            "r2c_rel_l2": O.rel_l2_rows(X[idx].cpu().numpy(), ref)}
+        del x, X, gx
+    torch.cuda.synchronize()
+    return out
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
@@ -430,6 +522,7 @@ def run_ours(args):
     if rank != 0:
         return 0
 
+    extras = extra_measurements(dev, stream) if world == 1 and not args.no_extras else None
     cpu = None
     if world == 1:
         threads = os.cpu_count() or 1
@@ -463,13 +556,16 @@ def run_ours(args):
         "clocks": clocks.summary() if clocks else None,
         "cpu_baseline": cpu,
     }
+    if extras:
+        line.update(extras)
     print(json.dumps(line), flush=True)
     return 0
 
 
 def run_case(spec: str, reps: int):
     """Launch one kernel configuration `reps` times without timing (for ncu captures):
-    spec = kind:n:batch with kind in c2c, c2c_inv, r2c, c2r."""
+    spec = kind:n:batch with kind in c2c, c2c_inv, tc2, tc3 (tensor-core splits), r2c, c2r,
+    or ragged:grid:CAP."""
     import torch
     import bfly
     kind, n, b = spec.split(":")
@@ -499,6 +595,10 @@ def run_case(spec: str, reps: int):
         x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
         y = torch.empty_like(x)
         call = lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, 1 if kind == "c2c_inv" else -1, 1.0, 0)
+    elif kind in ("tc2", "tc3"):
+        x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.empty_like(x)
+        call = lambda: plan.exec_c2c_tc(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, int(kind[2]), 0)
     elif kind == "r2c":
         x = torch.randn(b, n, device=dev, generator=g)
         y = torch.empty(b, n // 2 + 1, dtype=torch.complex64, device=dev)
@@ -522,6 +622,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default=None, help="kind:n:batch, launch only that kernel (for ncu)")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--no-extras", action="store_true", help="skip the split-BF16 / fwd+bwd sub-measurements")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
