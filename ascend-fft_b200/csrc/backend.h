@@ -82,8 +82,10 @@ int raggedStatus(unsigned* status, bool clear);
 // Split-BF16 tensor-core C2C (tcgen05): n in {256, 4096}, split = 2 or 3 bf16 terms; tw is the
 // Stockham table of (n, 16).
 bool hasTensorVariant(uint32_t n, int split);
+size_t tensorTableBytes(int split);                            // split DFT-16 operand
+int buildTensorTable(void* table, int split, void* stream);    // FP64 on the device
 int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
-                    const void* tw, int split, void* stream);
+                    const void* tw, const void* table, int split, void* stream);
 int tensorStatus(unsigned* status, bool clear);
 
 }  // namespace backend

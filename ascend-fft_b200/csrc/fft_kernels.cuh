@@ -69,24 +69,34 @@ k_r2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     float2* sm = smem + rl * S;
     float2 v[E];
     TM::run(v, sm, tw, t, rl, [&](int i) { return ok ? ld_stream(src + i) : make_float2(0.f, 0.f); });
+    // twiddles of this thread's output bins k = t + i*T (and bin M for t == 0), in flight
+    // while Z goes through shared memory
+    float2 w[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) w[i] = __ldg(twr + t + i * T);
+    const float2 wm = __ldg(twr + M);
     TM::sync(rl);
     TM::for_each_out(v, t, [&](int i, float2 x) { sm[spad(i)] = x; });
     TM::sync(rl);
     if (!ok) return;
-    for (int k = t; k <= M; k += T) {
+    auto bin = [&](int k, float2 wk) {
         const float2 a = sm[spad(k & (M - 1))];
         const float2 b = sm[spad((M - k) & (M - 1))];
         const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
         const float2 o = make_float2(0.5f * (a.y + b.y), 0.5f * (b.x - a.x));
-        float2 X = cadd(e, cmul<false>(o, __ldg(twr + k)));
+        float2 X = cadd(e, cmul<false>(o, wk));
         if constexpr (WEIGHTED) X = cscale(X, (k == 0 || k == M) ? s_edge : s_int);
         st_stream(dst + k, X);
-    }
+    };
+#pragma unroll
+    for (int i = 0; i < E; ++i) bin(t + i * T, w[i]);
+    if (t == 0) bin(M, wm);
 }
 
 // ------------------------------------------------------------------ C2R
-// X half spectrum [M+1] (M = N/2).  Imaginary parts of X[0] and X[M] are ignored, as in the
-// real part extraction of kfft_c2r_post (fft_real.cpp:262-263).  For k = 0..M-1:
+// X half spectrum [M+1] (M = N/2), staged once in shared memory.  Imaginary parts of X[0] and
+// X[M] are ignored, as in the real part extraction of kfft_c2r_post (fft_real.cpp:262-263).
+// For k = 0..M-1:
 //   Xk = X[k], Xm = X[M-k] (scaled by s_edge at DC/Nyquist, s_int elsewhere),
 //   Z[k] = (Xk + conj Xm) + i (Xk - conj Xm) W_N^-k,  z = IDFT_M(Z) * out_scale,
 //   x[2m] = Re z[m], x[2m+1] = Im z[m].   out_scale = 1/N gives numpy.fft.irfft.
@@ -105,10 +115,19 @@ k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     const bool ok = row < batch;
     const float2* src = in + row * (M + 1);
     float2* dst = out + row * M;
+    float2* sm = smem + rl * S;
+    // stage bins 0..M-1 once (coalesced), then pair bin k with bin M-k from shared memory; the
+    // Nyquist bin M pairs only with bin 0 and is read directly
+    const float2 nyq = (ok && t == 0) ? ld_stream(src + M) : make_float2(0.f, 0.f);   // before the barrier
     float2 v[E];
-    TM::run(v, smem + rl * S, tw, t, rl, [&](int k) {
-        if (!ok) return make_float2(0.f, 0.f);
-        float2 xk = __ldg(src + k), xm = __ldg(src + (M - k));
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = ok ? ld_stream(src + t + i * T) : make_float2(0.f, 0.f);   // all loads in flight
+#pragma unroll
+    for (int i = 0; i < E; ++i) sm[spad(t + i * T)] = v[i];
+    TM::sync(rl);
+    TM::load_first(v, t, [&](int k) {
+        float2 xk = sm[spad(k)];
+        float2 xm = k == 0 ? nyq : sm[spad(M - k)];
         if (k == 0) {
             xk = make_float2(xk.x * s_edge, 0.f);
             xm = make_float2(xm.x * s_edge, 0.f);
@@ -120,6 +139,8 @@ k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
         const float2 od = cmul<true>(make_float2(xk.x - xm.x, xk.y + xm.y), __ldg(twr + k));
         return make_float2((ev.x - od.y) * out_scale, (ev.y + od.x) * out_scale);
     });
+    TM::sync(rl);   // the passes reuse the staging buffer for their exchanges
+    TM::template passes<0>(v, sm, tw, t, rl);
     if (ok) TM::for_each_out(v, t, [&](int i, float2 x) { st_stream(dst + i, x); });
 }
 

@@ -49,10 +49,43 @@ __device__ __forceinline__ void split_terms(float v, float (&t)[SPLIT]) {
     }
 }
 
+// Split a pair of values into SPLIT packed bf16x2 terms (one conversion per term for both).
+template <int SPLIT>
+__device__ __forceinline__ void split_pair(float a, float b, uint32_t (&t)[SPLIT]) {
+    float ra = a, rb = b;
+#pragma unroll
+    for (int s = 0; s < SPLIT; ++s) {
+        const __nv_bfloat162 h = __float22bfloat162_rn(make_float2(ra, rb));
+        t[s] = *reinterpret_cast<const uint32_t*>(&h);
+        ra = ra - __low2float(h);
+        rb = rb - __high2float(h);
+    }
+}
+
+// The SPLIT bf16 terms of the 32 x 32 real DFT-16 matrix in the K-major canonical layout
+// (SPLIT x 2048 bytes), computed once in FP64: row n = output (Re y_0..15, Im y_0..15), column
+// k = input (Re x_0..15, Im x_0..15):
+//   Re y_n = sum_k c_nk Re x_k + s_nk Im x_k,  Im y_n = sum_k -s_nk Re x_k + c_nk Im x_k,
+//   c_nk = cos(2 pi n k / 16), s_nk = sin(2 pi n k / 16)
+template <int SPLIT>
+__global__ void k_tc_dft_table(unsigned char* __restrict__ table) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 32 * 32) return;
+    const int n = e >> 5, k = e & 31;
+    double sn, cs;
+    sincospi((double)(((n & 15) * (k & 15)) & 15) / 8.0, &sn, &cs);   // multiples of pi/8
+    const float v = (float)((n < 16) ? (k < 16 ? cs : sn) : (k < 16 ? -sn : cs));
+    float parts[SPLIT];
+    split_terms<SPLIT>(v, parts);
+#pragma unroll
+    for (int s = 0; s < SPLIT; ++s)
+        *reinterpret_cast<__nv_bfloat16*>(table + s * kBBytes + kmajor_offset(n, k)) = __float2bfloat16_rn(parts[s]);
+}
+
 template <int N, int SPLIT>
 __global__ void __launch_bounds__(kTcThreads, SPLIT == 2 ? 3 : 2)
 k_c2c_tc(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
-         uint64_t batch, int direction, float scale) {
+         const unsigned char* __restrict__ dftTable, uint64_t batch, int direction, float scale) {
     constexpr int E = 16;
     using Sd = Sched<N, E>;
     static_assert(Sd::radix(Sd::P - 1) == 16, "length must be a power of 16");
@@ -63,7 +96,7 @@ k_c2c_tc(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
     constexpr int NPROD = SPLIT == 2 ? 3 : 6;
 
     extern __shared__ __align__(1024) unsigned char smem_tc[];
-    unsigned char* aBase = smem_tc;                                 // [SPLIT][2 tiles][8 KB]
+    unsigned char* aBase = smem_tc;                                   // [SPLIT][2 tiles][8 KB]
     unsigned char* bBase = smem_tc + SPLIT * 2 * kTileBytes;          // [SPLIT][2 KB]
     float2* xbuf = reinterpret_cast<float2*>(bBase + SPLIT * kBBytes);
     uint64_t* bar = reinterpret_cast<uint64_t*>(xbuf + ROWS * S);
@@ -79,22 +112,9 @@ k_c2c_tc(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
         mbar_init(bar, 1);
         fence_mbar_init();
     }
-    // B terms: the 32 x 32 real DFT-16 matrix (forward), row n = output, column k = input.
-    //   Re y_n = sum_k c_nk Re x_k + s_nk Im x_k,  Im y_n = sum_k -s_nk Re x_k + c_nk Im x_k,
-    //   c_nk = cos(2 pi n k / 16), s_nk = sin(2 pi n k / 16)
-    for (int e = tid; e < 32 * 32; e += kTcThreads) {
-        const int n = e >> 5, k = e & 31;
-        const int nn = n & 15, kk = k & 15;
-        double sn, cs;
-        sincospi((double)((nn * kk) & 15) / 8.0, &sn, &cs);   // angles are multiples of pi/8
-        const float v = (float)((n < 16) ? (k < 16 ? cs : sn) : (k < 16 ? -sn : cs));
-        float parts[SPLIT];
-        split_terms<SPLIT>(v, parts);
-#pragma unroll
-        for (int s = 0; s < SPLIT; ++s)
-            *reinterpret_cast<__nv_bfloat16*>(bBase + s * kBBytes + kmajor_offset(n, k)) =
-                __float2bfloat16_rn(parts[s]);
-    }
+    // the DFT operand terms, built once per plan (k_tc_dft_table), copied into shared memory
+    for (int i = tid; i < SPLIT * kBBytes / 16; i += kTcThreads)
+        reinterpret_cast<uint4*>(bBase)[i] = __ldg(reinterpret_cast<const uint4*>(dftTable) + i);
     fence_proxy_async_smem();
     tc_fence_before_sync();
     __syncthreads();
@@ -103,108 +123,110 @@ k_c2c_tc(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
 
     const int rl = tid / T;
     const int j = tid - rl * T;
-    const uint64_t row = (uint64_t)blockIdx.x * ROWS + rl;
-    const bool ok = row < batch;
     const float sgn = direction > 0 ? -1.f : 1.f;
     const int tile = tid >> 7, m = tid & 127;
-    const float2* src = in + row * N;
-    float2* dst = out + row * N;
     float2* xr = xbuf + rl * S;
-    float2 v[16];
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {
-        float2 x = ok ? ld_stream(src + j + r * (N / 16)) : make_float2(0.f, 0.f);
-        v[r] = make_float2(x.x, sgn * x.y);
-    }
     constexpr uint32_t idesc = umma_idesc_bf16(128, 32);
+    const uint64_t groups = (batch + ROWS - 1) / ROWS;
     bool failed = false;
-    uint32_t pendingParity = 0;
+    uint32_t phase = 0;
 #pragma unroll 1
-    for (int p = 0; p < P; ++p) {
-        const int Ns = Sd::ns(p);
-        if (p > 0) {
-            const float2* twp = tw + Sd::twoff(p);
-            const int k = j & (Ns - 1);
+    for (uint64_t grp = blockIdx.x; grp < groups && !failed; grp += gridDim.x) {
+        const uint64_t row = grp * ROWS + rl;
+        const bool ok = row < batch;
+        const float2* src = in + row * N;
+        float2* dst = out + row * N;
+        float2 v[16];
 #pragma unroll
-            for (int r = 1; r < 16; ++r) v[r] = cmul<false>(v[r], __ldg(twp + (r - 1) * Ns + k));
+        for (int r = 0; r < 16; ++r) {
+            float2 x = ok ? ld_stream(src + j + r * (N / 16)) : make_float2(0.f, 0.f);
+            v[r] = make_float2(x.x, sgn * x.y);
         }
-        // A terms of this butterfly: row m of tile `tile`, K chunks of 8 (Re 0-7, Re 8-15, Im 0-7, Im 8-15)
+#pragma unroll 1
+        for (int p = 0; p < P; ++p) {
+            const int Ns = Sd::ns(p);
+            if (p > 0) {
+                const float2* twp = tw + Sd::twoff(p);
+                const int k = j & (Ns - 1);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            float pr[8][SPLIT];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int r = (c & 1) * 8 + e;
-                split_terms<SPLIT>(c < 2 ? v[r].x : v[r].y, pr[e]);
+                for (int r = 1; r < 16; ++r) v[r] = cmul<false>(v[r], __ldg(twp + (r - 1) * Ns + k));
             }
+            // A terms of this butterfly: row m of tile `tile`, K chunks (Re 0-7, Re 8-15, Im 0-7, Im 8-15)
 #pragma unroll
-            for (int s = 0; s < SPLIT; ++s) {
-                uint4 q;
-                q.x = pack_bf16(pr[0][s], pr[1][s]);
-                q.y = pack_bf16(pr[2][s], pr[3][s]);
-                q.z = pack_bf16(pr[4][s], pr[5][s]);
-                q.w = pack_bf16(pr[6][s], pr[7][s]);
-                *reinterpret_cast<uint4*>(aBase + (s * 2 + tile) * kTileBytes + kmajor_offset(m, c * 8)) = q;
-            }
-        }
-        fence_proxy_async_smem();
-        tc_fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            tc_fence_after_sync();
-            // products (A term, B term), smallest first
-            constexpr int pa[6] = {2, 1, 0, 1, 0, 0};
-            constexpr int pb[6] = {0, 1, 2, 0, 1, 0};
-            constexpr int pa2[3] = {1, 0, 0};
-            constexpr int pb2[3] = {0, 1, 0};
+            for (int c = 0; c < 4; ++c) {
+                uint32_t q[4][SPLIT];
 #pragma unroll
-            for (int tl = 0; tl < 2; ++tl) {
-#pragma unroll
-                for (int q = 0; q < NPROD; ++q) {
-                    const int sa = SPLIT == 2 ? pa2[q] : pa[q];
-                    const int sb = SPLIT == 2 ? pb2[q] : pb[q];
-#pragma unroll
-                    for (int ks = 0; ks < 2; ++ks) {
-                        const uint32_t aAddr = smem_addr(aBase + (sa * 2 + tl) * kTileBytes) + ks * 256;
-                        const uint32_t bAddr = smem_addr(bBase + sb * kBBytes) + ks * 256;
-                        umma_bf16(tmem + tl * 32, umma_smem_desc(aAddr, 128, 512), umma_smem_desc(bAddr, 128, 512),
-                                  idesc, q > 0 || ks > 0);
-                    }
+                for (int e = 0; e < 4; ++e) {
+                    const int r = (c & 1) * 8 + 2 * e;
+                    if (c < 2) split_pair<SPLIT>(v[r].x, v[r + 1].x, q[e]);
+                    else split_pair<SPLIT>(v[r].y, v[r + 1].y, q[e]);
                 }
+#pragma unroll
+                for (int s = 0; s < SPLIT; ++s)
+                    *reinterpret_cast<uint4*>(aBase + (s * 2 + tile) * kTileBytes + kmajor_offset(m, c * 8)) =
+                        make_uint4(q[0][s], q[1][s], q[2][s], q[3][s]);
             }
-            umma_commit(bar);
-        }
-        const bool done = mbar_wait_bounded(bar, (uint32_t)(p & 1));
-        if (__syncthreads_or(!done)) {
-            failed = true;
-            pendingParity = (uint32_t)(p & 1);
-            break;
-        }
-        tc_fence_after_sync();
-        float d[32];
-        tmem_ld_32cols(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(tile * 32), d);
-#pragma unroll
-        for (int r = 0; r < 16; ++r) v[r] = make_float2(d[r], d[16 + r]);
-        if (p < P - 1) {
-            const int k = j & (Ns - 1);
-            const int base = (j - k) * 16 + k;
-#pragma unroll
-            for (int r = 0; r < 16; ++r) xr[spad(base + r * Ns)] = v[r];
+            fence_proxy_async_smem();
             tc_fence_before_sync();
             __syncthreads();
+            if (tid == 0) {
+                tc_fence_after_sync();
+                // products (A term, B term), smallest first
+                constexpr int pa[6] = {2, 1, 0, 1, 0, 0};
+                constexpr int pb[6] = {0, 1, 2, 0, 1, 0};
+                constexpr int pa2[3] = {1, 0, 0};
+                constexpr int pb2[3] = {0, 1, 0};
 #pragma unroll
-            for (int r = 0; r < 16; ++r) v[r] = xr[spad(j + r * (N / 16))];
+                for (int tl = 0; tl < 2; ++tl) {
+#pragma unroll
+                    for (int q = 0; q < NPROD; ++q) {
+                        const int sa = SPLIT == 2 ? pa2[q] : pa[q];
+                        const int sb = SPLIT == 2 ? pb2[q] : pb[q];
+#pragma unroll
+                        for (int ks = 0; ks < 2; ++ks) {
+                            const uint32_t aAddr = smem_addr(aBase + (sa * 2 + tl) * kTileBytes) + ks * 256;
+                            const uint32_t bAddr = smem_addr(bBase + sb * kBBytes) + ks * 256;
+                            umma_bf16(tmem + tl * 32, umma_smem_desc(aAddr, 128, 512),
+                                      umma_smem_desc(bAddr, 128, 512), idesc, q > 0 || ks > 0);
+                        }
+                    }
+                }
+                umma_commit(bar);
+            }
+            const bool done = mbar_wait_bounded(bar, phase);
+            if (__syncthreads_or(!done)) {
+                failed = true;
+                break;
+            }
+            phase ^= 1u;
+            tc_fence_after_sync();
+            float d[32];
+            tmem_ld_32cols(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(tile * 32), d);
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = make_float2(d[r], d[16 + r]);
+            if (p < P - 1) {
+                const int k = j & (Ns - 1);
+                const int base = (j - k) * 16 + k;
+#pragma unroll
+                for (int r = 0; r < 16; ++r) xr[spad(base + r * Ns)] = v[r];
+                tc_fence_before_sync();
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < 16; ++r) v[r] = xr[spad(j + r * (N / 16))];
+            }
         }
+        if (!failed && ok) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+                st_stream(dst + j + r * (N / 16), make_float2(v[r].x * scale, sgn * scale * v[r].y));
+        }
+        // the exchange buffer and the A operand are rewritten by the next group
+        tc_fence_before_sync();
+        __syncthreads();
     }
-    if (failed) {
-        if (tid == 0) {
-            atomicOr(&g_tc_status, 1u);
-            mbar_wait_bounded(bar, pendingParity);   // let the MMAs in flight finish if they can
-        }
-    } else if (ok) {
-#pragma unroll
-        for (int r = 0; r < 16; ++r)
-            st_stream(dst + j + r * (N / 16), make_float2(v[r].x * scale, sgn * scale * v[r].y));
+    if (failed && tid == 0) {
+        atomicOr(&g_tc_status, 1u);
+        mbar_wait_bounded(bar, phase);   // let the MMAs in flight finish if they can
     }
     tc_fence_before_sync();
     __syncthreads();
@@ -223,31 +245,47 @@ namespace backend {
 
 template <int N, int SPLIT>
 static int launchTc(const void* in, void* out, uint64_t batch, bool inverse, float scale, const void* tw,
-                    void* stream) {
+                    const void* table, void* stream) {
     constexpr int smem = dev::tcSmemBytes<N, SPLIT>();
-    static bool attr = false;
-    if (!attr) {
+    static int resident = 0;   // CTAs resident on the whole device (persistent grid)
+    if (!resident) {
+        int dev = 0, sms = 0, perSm = 0;
         if (cudaFuncSetAttribute(dev::k_c2c_tc<N, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-            cudaSuccess)
+                cudaSuccess ||
+            cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, dev::k_c2c_tc<N, SPLIT>, dev::kTcThreads, smem) !=
+                cudaSuccess)
             return 1;
-        attr = true;
+        resident = sms * (perSm > 0 ? perSm : 1);
     }
     constexpr int rows = dev::kTcThreads / (N / 16);
-    const unsigned grid = (unsigned)((batch + rows - 1) / rows);
+    const uint64_t groups = (batch + rows - 1) / rows;
+    const unsigned grid = (unsigned)(groups < (uint64_t)resident ? groups : (uint64_t)resident);
     dev::k_c2c_tc<N, SPLIT><<<grid, dev::kTcThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw), batch,
-        inverse ? 1 : -1, scale);
+        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw),
+        static_cast<const unsigned char*>(table), batch, inverse ? 1 : -1, scale);
     return (int)cudaGetLastError();
 }
 
 bool hasTensorVariant(uint32_t n, int split) { return (n == 256 || n == 4096) && (split == 2 || split == 3); }
 
+size_t tensorTableBytes(int split) { return (size_t)split * dev::kBBytes; }
+
+int buildTensorTable(void* table, int split, void* stream) {
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (split == 2) dev::k_tc_dft_table<2><<<4, 256, 0, st>>>(static_cast<unsigned char*>(table));
+    else if (split == 3) dev::k_tc_dft_table<3><<<4, 256, 0, st>>>(static_cast<unsigned char*>(table));
+    else return (int)cudaErrorInvalidValue;
+    return (int)cudaGetLastError();
+}
+
 int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
-                    const void* tw, int split, void* stream) {
-    if (n == 256 && split == 2) return launchTc<256, 2>(in, out, batch, inverse, scale, tw, stream);
-    if (n == 256 && split == 3) return launchTc<256, 3>(in, out, batch, inverse, scale, tw, stream);
-    if (n == 4096 && split == 2) return launchTc<4096, 2>(in, out, batch, inverse, scale, tw, stream);
-    if (n == 4096 && split == 3) return launchTc<4096, 3>(in, out, batch, inverse, scale, tw, stream);
+                    const void* tw, const void* table, int split, void* stream) {
+    if (n == 256 && split == 2) return launchTc<256, 2>(in, out, batch, inverse, scale, tw, table, stream);
+    if (n == 256 && split == 3) return launchTc<256, 3>(in, out, batch, inverse, scale, tw, table, stream);
+    if (n == 4096 && split == 2) return launchTc<4096, 2>(in, out, batch, inverse, scale, tw, table, stream);
+    if (n == 4096 && split == 3) return launchTc<4096, 3>(in, out, batch, inverse, scale, tw, table, stream);
     return (int)cudaErrorInvalidValue;
 }
 

@@ -341,6 +341,7 @@ struct Plan::Impl {
     size_t devInCap = 0, devOutCap = 0, devWorkCap = 0;
     backend::Timer* timer = nullptr;
     void* aux[2] = {nullptr, nullptr};   // extra streams of the pipelined host round trip
+    void* tcTable[4] = {nullptr, nullptr, nullptr, nullptr};   // split DFT-16 operand per term count
 };
 
 Plan::Plan(Candidate c) : cand_(std::move(c)) {}
@@ -359,6 +360,8 @@ Plan::~Plan() {
     backend::timerDestroy(impl_->timer);
     for (void* st : impl_->aux)
         if (st) backend::streamDestroy(st);
+    for (void* t : impl_->tcTable)
+        if (t) backend::release(t);
 }
 
 static int ensureBuf(void** p, size_t* cap, size_t bytes) {
@@ -534,8 +537,18 @@ int Plan::execC2CTensor(const void* dIn, void* dOut, uint32_t n, uint64_t batch,
         (direction != -1 && direction != 1) || !backend::hasTensorVariant(n, splitTerms))
         return -8;
     if (prepareC2C(n, 16)) return -2;
-    if (backend::launchC2CTensor(dIn, dOut, n, batch, direction > 0, scale, impl_->twC2C[{n, 16}], splitTerms,
-                                 stream))
+    void*& table = impl_->tcTable[splitTerms];
+    if (!table) {
+        void* t = nullptr;
+        if (backend::alloc(&t, backend::tensorTableBytes(splitTerms))) return -3;
+        if (backend::buildTensorTable(t, splitTerms, stream_) || backend::streamSync(stream_)) {
+            backend::release(t);
+            return -2;
+        }
+        table = t;
+    }
+    if (backend::launchC2CTensor(dIn, dOut, n, batch, direction > 0, scale, impl_->twC2C[{n, 16}], table,
+                                 splitTerms, stream))
         return -5;
     return 0;
 }
@@ -573,11 +586,11 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
 }
 
 // Body of the synchronous host-pointer entry points: upload, enqueue, synchronise, download.
-// Batches above kPipelineBytes are cut into row chunks of about kChunkBytes that rotate over
+// Transfers above kPipelineBytes are cut into row chunks of about kChunkBytes that rotate over
 // three streams, so the H2D of one chunk, the kernels of another and the D2H of a third
 // overlap (two copy engines).  enqueue() returns an exec status: -2 prepare and -3 alloc pass
 // through, any other failure is a launch failure (-5).
-constexpr size_t kPipelineBytes = 16u << 20, kChunkBytes = 8u << 20;
+constexpr size_t kPipelineBytes = 4u << 20, kChunkBytes = 4u << 20;
 
 template <class Enqueue>
 int Plan::roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRowBytes,

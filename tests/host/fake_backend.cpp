@@ -165,8 +165,10 @@ int launchRaggedFlat(const void* entries, int count, const void*, uint64_t tiles
 }
 
 bool hasTensorVariant(uint32_t n, int split) { return (n == 256 || n == 4096) && (split == 2 || split == 3); }
+size_t tensorTableBytes(int split) { return (size_t)split * 2048; }
+int buildTensorTable(void*, int, void*) { return launch(); }
 int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
-                    const void* tw, int, void* s) {
+                    const void* tw, const void*, int, void* s) {
     return launchC2C(in, out, n, batch, inverse, scale, tw, 16, 256, s);
 }
 int tensorStatus(unsigned* status, bool) { *status = 0; return 0; }

@@ -272,7 +272,7 @@ int main(int argc, char** argv) {
 
     // ---- large batch: the round trip is pipelined over row chunks on three streams
     {
-        const uint32_t bn = 64, bb = 17000;   // 2 x 8.7 MB > 16 MB pipelining threshold
+        const uint32_t bn = 64, bb = 17000;   // 2 x 8.7 MB > 4 MB pipelining threshold
         std::vector<float> bin(2 * (size_t)bn * bb), bout(bin.size()), bref(2 * bn);
         for (size_t i = 0; i < bin.size(); ++i) bin[i] = bfly::patternAt(i * 3 + 1);
         const int streamsBefore = fake::streamsCreated;
@@ -284,7 +284,7 @@ int main(int argc, char** argv) {
             bfly::refFftF32(bin.data() + (size_t)rows[i] * 2 * bn, bref.data(), bn);
             CHECK(bfly::maxRelScaled(bout.data() + (size_t)rows[i] * 2 * bn, bref.data(), 2 * bn) < 1e-5);
         }
-        fake::failCopy = fake::copies + 3;   // the second chunk's upload
+        fake::failCopy = fake::copies + 3;   // the second chunk's upload (4 MB chunks: 8192 rows)
         const int rc = plan->run(bin.data(), bout.data(), bn, bb);
         CHECK(rc == -4);
         fake::failCopy = 0;
