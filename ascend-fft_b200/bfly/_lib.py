@@ -48,6 +48,7 @@ SIGNATURES = {
     "bfly_plan_exec_c2c_tc_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
                                               C.c_int, C.c_float, C.c_int, C.c_void_p]),
     "bfly_tc_device_status": (C.c_int, [C.POINTER(C.c_uint)]),
+    "bfly_long_device_status": (C.c_int, [C.POINTER(C.c_uint)]),
     "bfly_ragged_create": (C.c_int, [c_plan, C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]),
     "bfly_ragged_exec_async": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfly_ragged_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int),

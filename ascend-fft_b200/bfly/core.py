@@ -172,6 +172,14 @@ class Plan:
             raise BflyError("bfly_tc_device_status", rc)
         return st.value
 
+    def long_device_status(self) -> int:
+        """Error word of the single-pass cluster long C2C (0 = clean); reading clears it."""
+        st = C.c_uint()
+        rc = self._lib.bfly_long_device_status(C.byref(st))
+        if rc:
+            raise BflyError("bfly_long_device_status", rc)
+        return st.value
+
     def make_ragged(self, requests):
         """requests: iterable of (d_in, d_out, n, batch, direction, scale) with device
         pointers; returns a Ragged whose exec(stream) is one persistent kernel launch."""

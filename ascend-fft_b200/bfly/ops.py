@@ -32,7 +32,7 @@ BEST_C2C = {32: "r8_cta256_shared_fp32_stockham", 64: "r8_cta256_shared_fp32_sto
             128: "r16_cta128_shared_fp32_stockham", 256: "r16_cta128_shared_fp32_stockham",
             512: "r16_cta128_shared_fp32_stockham", 1024: "r16_cta256_shared_fp32_stockham",
             2048: "r16_cta128_shared_fp32_stockham", 4096: "r16_cta256_shared_fp32_stockham",
-            8192: "r16_cta512_shared_fp32_stockham"}
+            8192: "r16_cta512_shared_fp32_stockham", 16384: "r16_cta1024_shared_fp32_stockham"}
 BEST_REAL = {32: "r8_cta256_shared_fp32_stockham", 64: "r8_cta256_shared_fp32_stockham",
              128: "r16_cta128_shared_fp32_stockham", 256: "r16_cta128_shared_fp32_stockham",
              512: "r16_cta128_shared_fp32_stockham", 1024: "r16_cta128_shared_fp32_stockham",
@@ -71,7 +71,9 @@ def plan_for(device: torch.device, n: int | None = None, kind: str = "c2c"):
     table = BEST_C2C if kind == "c2c" else BEST_REAL
     key = n if kind == "c2c" else (n // 2 if n else None)
     cid = table.get(key, DEFAULT_CANDIDATE) if key is not None else DEFAULT_CANDIDATE
-    return _plan_by_id(st, cid, 1024)   # every tabled candidate is feasible at 1024
+    # a C2C entry is feasible at its own length (16384 has only the 1024-thread kernel); the
+    # real-transform entries, keyed by n/2, and the default are all feasible at 1024
+    return _plan_by_id(st, cid, n if kind == "c2c" and n in BEST_C2C else 1024)
 
 
 def autotune(n: int, batch: int, device: torch.device | None = None, top_k: int = 3,

@@ -64,6 +64,17 @@ int launchLongA(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
 int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t batch,
                 bool inverse, float scale, const void* tw2, void* stream);
 
+// Single-pass long C2C: one thread-block cluster per row, transpose through distributed
+// shared memory (n in 8192..65536; tw1 = Stockham (n/256, 16), tw2 = Stockham (256, 16)).
+// `cta` threads per CTA (256, or 512 for n >= 16384) sets the cluster size n / (16 * cta).
+// Returns kLongClusterUnaligned (nothing launched) when `in` is not 16-byte aligned, which the
+// TMA tensor map needs; callers then use the four-step kernels.
+constexpr int kLongClusterUnaligned = 0x4c43;
+bool hasLongCluster(uint32_t n, int cta);
+int launchLongCluster(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+                      const void* tw1, const void* tw2, const void* tlo, const void* thi, int cta, void* stream);
+int longClusterStatus(unsigned* status, bool clear);   // device error word of the cluster kernel; 0 on success
+
 // Ragged persistent launch over a device array of RaggedEntry (ragged.h).
 int raggedSmemBytes();
 int raggedGrid(int device, int* grid);   // resident CTAs on the whole device

@@ -188,6 +188,7 @@ int bfly_plan_exec_c2c_tc_async(bfly_plan* plan, const void* d_in, void* d_out, 
 }
 
 int bfly_tc_device_status(unsigned* status) { return bfly::Plan::tensorStatus(status); }
+int bfly_long_device_status(unsigned* status) { return bfly::Plan::longStatus(status); }
 
 int bfly_ragged_create(bfly_plan* plan, const bfly_ragged_request* reqs, size_t count,
                        bfly_ragged** out) {

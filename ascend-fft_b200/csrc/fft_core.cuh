@@ -222,12 +222,19 @@ __host__ __device__ constexpr int sync_kind(int T, int ctaThreads) {
 // `sm` is this transform's exchange buffer (smem_stride<> float2), `tw` the Stockham
 // twiddle table of Sched<N,E> (TWSIZE entries, pass p at twoff(p)), `load(i)` yields input
 // element i.  SYNC selects the barrier (see team_sync); `row` is the transform's index in its
-// CTA (named-barrier id - 1).
-template <int N, int E, bool INV, int SYNC>
+// CTA (named-barrier id - 1).  ESTRIDE selects the exchange layout: 0 = element i at
+// sm[spad(i)] (padded, threads of one transform across lanes); s > 0 = element i at sm[i*s]
+// (transforms across lanes, e.g. the columns of a tile staged densely by TMA).
+template <int N, int E, bool INV, int SYNC, int ESTRIDE = 0>
 struct Team {
     using S = Sched<N, E>;
     static constexpr int T = S::T;
     static constexpr int P = S::P;
+
+    static __device__ __forceinline__ int at(int i) {
+        if constexpr (ESTRIDE == 0) return spad(i);
+        else return i * ESTRIDE;
+    }
 
     static __device__ __forceinline__ void sync(int row) { team_sync<SYNC>(row, T); }
 
@@ -266,7 +273,7 @@ struct Team {
                 const int k = j & (Ns - 1);
                 const int base = (j - k) * R + k;
 #pragma unroll
-                for (int r = 0; r < R; ++r) sm[spad(base + r * Ns)] = v[s * R + r];
+                for (int r = 0; r < R; ++r) sm[at(base + r * Ns)] = v[s * R + r];
             }
             sync(row);
             constexpr int R2 = S::radix(p + 1);
@@ -274,7 +281,7 @@ struct Team {
 #pragma unroll
             for (int s = 0; s < B2; ++s)
 #pragma unroll
-                for (int r = 0; r < R2; ++r) v[s * R2 + r] = sm[spad(t + s * T + r * (N / R2))];
+                for (int r = 0; r < R2; ++r) v[s * R2 + r] = sm[at(t + s * T + r * (N / R2))];
             if constexpr (p + 1 < P - 1) sync(row);   // next pass writes the buffer again
             passes<p + 1>(v, sm, tw, t, row);
         }
@@ -292,6 +299,17 @@ struct Team {
                                                Load&& load) {
         load_first(v, t, load);
         passes<0>(v, sm, tw, t, row);
+    }
+
+    // Apply f(index, value&) to every output element held by this thread (in place).
+    template <class F>
+    static __device__ __forceinline__ void for_each_slot(float2 (&v)[E], int t, F&& f) {
+        constexpr int R = S::radix(P - 1);
+        constexpr int B = E / R;
+#pragma unroll
+        for (int s = 0; s < B; ++s)
+#pragma unroll
+            for (int r = 0; r < R; ++r) f(t + s * T + r * (N / R), v[s * R + r]);
     }
 
     // Apply f(index, value) to every output element held by this thread.

@@ -25,8 +25,14 @@ namespace bfly {
 namespace dev {
 
 // ------------------------------------------------------------------ C2C
+// Minimum resident CTAs that keeps a kernel at <= 64 registers per thread: the budget at which
+// the 512-thread single-transform kernels still fit two CTAs per SM.
+__host__ __device__ constexpr int min_blocks_64regs(int threads) {
+    return 65536 / (threads * 64) > 0 ? 65536 / (threads * 64) : 1;
+}
+
 template <int N, int E, int ROWS, bool INV>
-__global__ void __launch_bounds__((N / E) * ROWS)
+__global__ void __launch_bounds__((N / E) * ROWS, min_blocks_64regs((N / E) * ROWS))
 k_c2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
       uint64_t batch, float scale) {
     constexpr int T = N / E;

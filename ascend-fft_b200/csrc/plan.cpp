@@ -160,7 +160,7 @@ DesignSpace DesignSpace::load(const std::string& path) {
     stringAxis(l, "in", &sp.layoutsIn, {"interleaved", "planar"});
     stringAxis(l, "out", &sp.layoutsOut, {"interleaved", "planar"});
     stringAxis(f, "precision", &sp.precisions, {"fp32", "split_bf16"});
-    stringAxis(f, "schedule", &sp.schedules, {"stockham", "four_step"});
+    stringAxis(f, "schedule", &sp.schedules, {"stockham", "four_step", "cluster"});
     return sp;
 }
 
@@ -201,6 +201,7 @@ Metric estimate(const Hardware& hw, const Candidate& c, uint32_t n, uint32_t bat
     const int passes = loge ? (logn + loge - 1) / loge : logn;
     double us = 2.5 + hbmUs * (1.0 + 0.04 * std::max(0, passes - 2));
     if (c.f.schedule == "four_step") us = 3.0 + 2.0 * hbmUs;
+    if (c.f.schedule == "cluster") us = 3.0 + 1.3 * hbmUs;
     if (c.a.ctaThreads < 256) us *= 1.02;
     m.etaUs = us;
     return m;
@@ -269,6 +270,12 @@ std::vector<Candidate> enumerate(const DesignSpace& sp, const Hardware& hw, uint
             infeasible("fusion_level!=1 is not lowered (each schedule fuses all of its passes)");
         } else if (prec != "fp32") {
             infeasible("split_bf16 is served by the tensor-core entry points, not by plan candidates");
+        } else if (sched == "cluster") {
+            if (n < 8192) infeasible("cluster schedule is only used for n >= 8192");
+            else if (radix != 16) infeasible("cluster kernels use radix 16");
+            else if (!backend::hasLongCluster(n, cta))
+                infeasible("no cluster kernel for this (n, cta_threads): 256 threads per CTA, or 512 for n >= 16384");
+            else c.state = State::Unverified;
         } else if (sched == "four_step") {
             uint32_t n1 = 0, n2 = 0;
             backend::longSplit(n, &n1, &n2);
@@ -319,7 +326,8 @@ static bool lowerable(const Candidate& c, const Hardware& hw) {
     return c.a.validate(hw, nullptr) && c.p.coefficientResidency && c.p.fusionLevel == 1 &&
            (c.p.radix == 8 || c.p.radix == 16) && c.l.contiguous &&
            c.l.in == Layout::Interleaved && c.l.out == Layout::Interleaved &&
-           c.f.precision == "fp32" && (c.f.schedule == "stockham" || c.f.schedule == "four_step") &&
+           c.f.precision == "fp32" &&
+           (c.f.schedule == "stockham" || c.f.schedule == "four_step" || c.f.schedule == "cluster") &&
            (c.a.ctaThreads == 128 || c.a.ctaThreads == 256 || c.a.ctaThreads == 512 ||
             c.a.ctaThreads == 1024);
 }
@@ -402,17 +410,24 @@ bool Plan::validShape(uint32_t n, uint32_t batch, int kind) const {
     return resolve(rk, n, &e, &cta) == 0;
 }
 
-// Kernel variant for (kind, n): the candidate's radix/cta when compiled for n; C2C lengths past
-// the single-pass envelope (or candidates scheduled four_step) use the four-step kernels
-// (reported as e = 0).
+// Kernel variant for (kind, n): the candidate's radix/cta when compiled for n (one CTA per
+// transform, e = radix); otherwise, for long C2C lengths, the four-step kernels (e = 0), or one
+// thread-block cluster per row (e = -1) when the candidate is scheduled "cluster".  Measured on
+// B200 at batch*n = 2^26 the two-kernel four-step is the faster of the two at every long n
+// (the cluster kernel is bound by instruction issue at 16 resident warps per SM), so it is
+// the default.
 int Plan::resolve(int kind, uint32_t n, int* e, int* cta) const {
     const int r = cand_.p.radix, c = cand_.a.ctaThreads;
     if (kind == backend::kC2C) {
-        const bool wantLong = cand_.f.schedule == "four_step" || n > kMaxSinglePass ||
-                              !backend::hasVariant(backend::kC2C, n, r, c);
-        if (!wantLong) {
+        const std::string& sched = cand_.f.schedule;
+        if (sched == "stockham" && n <= kMaxSinglePass && backend::hasVariant(backend::kC2C, n, r, c)) {
             *e = r;
             *cta = c;
+            return 0;
+        }
+        if (sched == "cluster" && backend::hasLongCluster(n, 256)) {
+            *e = -1;
+            *cta = backend::hasLongCluster(n, c) ? c : 256;
             return 0;
         }
         uint32_t n1 = 0, n2 = 0;
@@ -486,12 +501,13 @@ int Plan::prepare(uint32_t n, uint32_t batch) {
     if (!validShape(n, batch, kPrepare)) return -8;
     int e = 0, cta = 0;
     if (resolve(backend::kC2C, n, &e, &cta)) return -8;
-    const int rcode = e ? prepareC2C(n, e) : prepareLong(n);
+    const int rcode = e > 0 ? prepareC2C(n, e) : prepareLong(n);
     if (rcode) return -1;
     tf_.clear();
     tf_.push_back({Transform::GenTwiddles, "FP64 twiddle tables built on the device, rounded to fp32"});
-    tf_.push_back({Transform::LaunchKernel, e ? "stockham single-pass kernel on the context stream"
-                                              : "four-step column + row kernels on the context stream"});
+    tf_.push_back({Transform::LaunchKernel, e > 0 ? "stockham single-pass kernel on the context stream"
+                                            : e < 0 ? "one thread-block cluster per row (on-chip transpose)"
+                                                    : "four-step column + row kernels on the context stream"});
     return 0;
 }
 
@@ -510,7 +526,7 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
     const bool inv = direction > 0;
     int e = 0, cta = 0;
     resolve(backend::kC2C, n, &e, &cta);
-    if (e) {
+    if (e > 0) {
         if (prepareC2C(n, e)) return -2;
         if (backend::launchC2C(dIn, dOut, n, batch, inv, scale, impl_->twC2C[{n, e}], e, cta, s)) return -5;
         return 0;
@@ -518,6 +534,15 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
     if (prepareLong(n)) return -2;
     uint32_t n1 = 0, n2 = 0;
     backend::longSplit(n, &n1, &n2);
+    if (e < 0) {
+        const auto& lt = impl_->twLong[n];
+        const int E = backend::longE();
+        const int rc = backend::launchLongCluster(dIn, dOut, n, batch, inv, scale, impl_->twC2C[{n1, E}],
+                                                  impl_->twC2C[{n2, E}], lt.lo, lt.hi, cta, s);
+        if (rc == 0) return 0;
+        if (rc != backend::kLongClusterUnaligned) return -5;
+        // an input the tensor map cannot address: the four-step kernels below take any float2 pointer
+    }
     if (!work) {
         if (ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
         work = impl_->devWork;
@@ -556,6 +581,11 @@ int Plan::execC2CTensor(const void* dIn, void* dOut, uint32_t n, uint64_t batch,
 int Plan::tensorStatus(unsigned* status) {
     if (!status) return -10;
     return backend::tensorStatus(status, true) ? -6 : 0;
+}
+
+int Plan::longStatus(unsigned* status) {
+    if (!status) return -10;
+    return backend::longClusterStatus(status, true) ? -6 : 0;
 }
 
 int Plan::execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
@@ -658,11 +688,11 @@ int Plan::runLong(const float* in, float* out, uint32_t n, uint32_t batch, int d
     if (prepare(n, batch)) return -2;
     int e = 0, cta = 0;
     resolve(backend::kC2C, n, &e, &cta);
-    if (!e && ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
+    if (e == 0 && ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
     // chunks on different streams use disjoint slices of the four-step workspace
     return roundTrip(in, (size_t)n * 8, out, (size_t)n * 8, batch,
                      [&](void* di, void* dout, uint32_t r0, uint32_t rows, void* st) {
-                         void* work = e ? nullptr : static_cast<char*>(impl_->devWork) + (size_t)r0 * n * 8;
+                         void* work = e != 0 ? nullptr : static_cast<char*>(impl_->devWork) + (size_t)r0 * n * 8;
                          return execC2CWith(di, dout, n, rows, direction, 1.0f, st, work);
                      });
 }

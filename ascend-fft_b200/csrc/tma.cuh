@@ -1,10 +1,12 @@
-// Bulk-copy (TMA) and mbarrier helpers for sm_100a, inline PTX.
+// Bulk-copy (TMA), mbarrier and thread-block-cluster helpers for sm_100a, inline PTX.
 //
-// Only the untiled bulk copy global -> shared of one contiguous span is used (no tensor map,
-// no multicast): both addresses 16-byte aligned, size a multiple of 16 bytes and below the
-// mbarrier transaction limit (2^20 - 1 bytes).  Every wait is bounded: a wait that has not
-// completed after kWaitNs of %globaltimer (or kWaitIters polls) reports failure so the kernel
-// can record an error and leave instead of hanging.
+// Copies: the untiled bulk copy of one contiguous span (both addresses 16-byte aligned, size a
+// multiple of 16 bytes) and the 2-D tiled tensor copy (tensor map built on the host; the
+// innermost coordinate times the element size is a multiple of 16 bytes, the shared-memory
+// destination 128-byte aligned).  Both complete transactions on an mbarrier (below its
+// 2^20 - 1 byte limit).  No multicast form is used anywhere.  Every wait is bounded: a wait
+// that has not completed after kWaitNs of %globaltimer (or kWaitIters polls) reports failure
+// so the kernel can record an error and leave instead of hanging.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -74,6 +76,67 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if ((i & 255u) == 255u && global_timer_ns() - t0 > kWaitNs) return false;
     }
     return false;
+}
+
+// try_wait with cluster-scope acquire: the phase was completed by st.async writes of other
+// CTAs of the cluster, whose data must be visible to this thread afterwards.
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_t parity) {
+    const uint64_t t0 = global_timer_ns();
+    for (uint32_t i = 0; i < kWaitIters; ++i) {
+        if (mbar_try_wait_cluster(bar, parity)) return true;
+        if ((i & 255u) == 255u && global_timer_ns() - t0 > kWaitNs) return false;
+    }
+    return false;
+}
+
+// 2-D tiled tensor copy global -> this CTA's shared memory (no multicast): box origin
+// (x, y) in elements of the tensor map, completion counted on `bar`.
+__device__ __forceinline__ void tensor_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_addr(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// ------------------------------------------------------------------ thread-block clusters
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// Split cluster barrier: arrive (release: this thread's earlier memory accesses are ordered
+// before the barrier) ... wait (acquire).  Every thread of the cluster alternates them.
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire;" ::: "memory"); }
+
+// Address of the same shared-memory location in CTA `rank` of this cluster.
+__device__ __forceinline__ uint32_t cluster_map(uint32_t saddr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+
+// Asynchronous 8-byte store into another CTA's shared memory that completes 8 transaction
+// bytes on that CTA's mbarrier (both addresses from cluster_map).  The sender does not wait.
+__device__ __forceinline__ void st_async_f2(uint32_t raddr, float2 v, uint32_t rbar) {
+    // No "memory" clobber: ordering against this CTA's other accesses comes from the cluster
+    // barrier and mbarrier waits around the sends, which carry one.
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(raddr),
+                 "f"(v.x), "f"(v.y), "r"(rbar));
 }
 
 }  // namespace dev

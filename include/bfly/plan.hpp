@@ -206,6 +206,7 @@ public:
                       float scale, int splitTerms, void* stream);
     // Device status of the tensor-core launches: 0, or 1 when a bounded MMA wait ran out.
     static int tensorStatus(unsigned* status);
+    static int longStatus(unsigned* status);   // cluster long-C2C kernel, same convention
 
     // Build a ragged persistent launch over `count` requests; *status receives 0 or a code
     // (-8 invalid request, -2 table build, -3 alloc, -4 upload, -1 runtime).

@@ -141,6 +141,21 @@ int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
     return 0;
 }
 
+bool hasLongCluster(uint32_t n, int cta) {
+    return (n == 8192 && cta == 256) || ((n == 16384 || n == 32768 || n == 65536) && (cta == 256 || cta == 512));
+}
+int launchLongCluster(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+                      const void*, const void*, const void*, const void*, int cta, void*) {
+    if (!hasLongCluster(n, cta)) return 1;
+    if (reinterpret_cast<uintptr_t>(in) % 16 != 0) return kLongClusterUnaligned;
+    if (int r = launch()) return r;
+    for (uint64_t b = 0; b < batch; ++b)
+        dft((const float*)in + b * 2 * n, (float*)out + b * 2 * n, n, inverse ? 1 : -1, scale);
+    return 0;
+}
+
+int longClusterStatus(unsigned* status, bool) { *status = 0; return 0; }
+
 int raggedSmemBytes() { return 34816; }
 int raggedGrid(int, int* grid) { *grid = 148 * 2; return 0; }
 int launchRagged(const void* entries, int count, uint64_t, int, void*) {

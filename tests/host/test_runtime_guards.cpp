@@ -79,12 +79,12 @@ int main(int argc, char** argv) {
         CHECK(invalid.init(badHw, space, "builtin") == -4);
     }
     for (const auto& bad : {std::string("{"), std::string("{}"), spText + " trailing",
-                            replaced(spText, "\"cta_threads\": [128, 256, 512]", "\"cta_threads\": []"),
-                            replaced(spText, "\"cta_threads\": [128, 256, 512]", "\"cta_threads\": [100]"),
+                            replaced(spText, "\"cta_threads\": [128, 256, 512, 1024]", "\"cta_threads\": []"),
+                            replaced(spText, "\"cta_threads\": [128, 256, 512, 1024]", "\"cta_threads\": [100]"),
                             replaced(spText, "\"radix\": [8, 16]", "\"radix\": [\"8\"]"),
                             replaced(spText, "\"radix\": [8, 16]", "\"radix\": [3]"),
                             replaced(spText, "\"out\": [\"interleaved\", \"planar\"]", "\"out\": [\"bogus\"]"),
-                            replaced(spText, "\"schedule\": [\"stockham\", \"four_step\"]", "\"schedule\": [\"fast\"]")}) {
+                            replaced(spText, "\"schedule\": [\"stockham\", \"cluster\", \"four_step\"]", "\"schedule\": [\"fast\"]")}) {
         write(badSp, bad);
         CHECK(throws([&] { bfly::DesignSpace::load(badSp); }));
         bfly::Context invalid;
@@ -155,7 +155,7 @@ int main(int argc, char** argv) {
         if (c.a.localExchange != "shared" || c.l.in != bfly::Layout::Interleaved ||
             c.l.out != bfly::Layout::Interleaved)
             CHECK(c.state == bfly::State::Infeasible && !c.reason.empty());
-        if (c.f.schedule == "four_step") CHECK(c.state == bfly::State::Infeasible);   // n <= 4096
+        if (c.f.schedule != "stockham") CHECK(c.state == bfly::State::Infeasible);   // n <= 4096
     }
     CHECK(feasible > 0);
 
@@ -179,15 +179,31 @@ int main(int argc, char** argv) {
         for (const auto& c : context.enumerate(4096, 524287)) live = live || c.state != bfly::State::Infeasible;
         CHECK(live);
     }
-    {   // long lengths: four-step feasible, single pass only up to 16384
-        int fs = 0, sp = 0;
+    {   // long lengths: four-step and cluster feasible, single CTA only up to 16384
+        int fs = 0, cl = 0, sp = 0;
         for (const auto& c : context.enumerate(65536, 4))
-            if (c.state != bfly::State::Infeasible) (c.f.schedule == "four_step" ? fs : sp)++;
-        CHECK(fs == 1 && sp == 0);
+            if (c.state != bfly::State::Infeasible)
+                (c.f.schedule == "four_step" ? fs : c.f.schedule == "cluster" ? cl : sp)++;
+        CHECK(fs == 1 && cl == 2 && sp == 0);   // cluster: 256- and 512-thread CTAs
         bool single8192 = false;
         for (const auto& c : context.enumerate(8192, 4))
             single8192 = single8192 || (c.state != bfly::State::Infeasible && c.f.schedule == "stockham");
         CHECK(single8192);
+        // which kernels prepare() lowers a 65536-point C2C to, per schedule
+        auto launchLabel = [&](const std::string& sched) {
+            for (const auto& c : context.enumerate(65536, 4))
+                if (c.state != bfly::State::Infeasible && c.f.schedule == sched) {
+                    auto pl = context.makePlan(c);
+                    if (!pl || pl->prepare(65536, 2) != 0) return std::string("<no plan>");
+                    for (const auto& t : pl->transforms())
+                        if (t.kind == bfly::Transform::LaunchKernel) return t.label;
+                }
+            return std::string("<none>");
+        };
+        CHECK(launchLabel("cluster").find("cluster") != std::string::npos);
+        CHECK(launchLabel("four_step").find("four-step") != std::string::npos);
+        CHECK(fake::allocations == fake::releases && fake::launches > 0);   // plans freed their tables
+        fake::allocations = fake::releases = fake::copies = fake::launches = 0;
     }
 
     // ---- guards: -8 before any allocation, copy or launch
