@@ -58,7 +58,7 @@ k_c2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
 // Optional per-bin weights (WEIGHTED): X[k] *= (k==0||k==M ? s_edge : s_int); used by the
 // adjoint of C2R.
 template <int N, int E, int ROWS, bool WEIGHTED>
-__global__ void __launch_bounds__((N / 2 / E) * ROWS)
+__global__ void __launch_bounds__((N / 2 / E) * ROWS, min_blocks_64regs((N / 2 / E) * ROWS))
 k_r2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
       const float2* __restrict__ twr, uint64_t batch, float s_edge, float s_int) {
     constexpr int M = N / 2;
@@ -107,7 +107,7 @@ k_r2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
 //   Z[k] = (Xk + conj Xm) + i (Xk - conj Xm) W_N^-k,  z = IDFT_M(Z) * out_scale,
 //   x[2m] = Re z[m], x[2m+1] = Im z[m].   out_scale = 1/N gives numpy.fft.irfft.
 template <int N, int E, int ROWS>
-__global__ void __launch_bounds__((N / 2 / E) * ROWS)
+__global__ void __launch_bounds__((N / 2 / E) * ROWS, min_blocks_64regs((N / 2 / E) * ROWS))
 k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
       const float2* __restrict__ twr, uint64_t batch, float s_edge, float s_int, float out_scale) {
     constexpr int M = N / 2;

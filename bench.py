@@ -283,9 +283,11 @@ def run_reference(args):
 # ------------------------------------------------------------------ our arm
 def extra_measurements(dev, stream):
     """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores vs fp32 at the
-    largest power-of-16 grid points; long C2C forward + backward (four-step, batch*n = 2^26);
+    largest power-of-16 grid points; long C2C forward + backward (batch*n = 2^26; single pass up
+    to n = 16384, four-step above);
     real transforms forward + adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
-    events on `stream` (20 launches after 3 warm-ups) and the error against FP64 on sampled rows."""
+    events on `stream` around one replay of a CUDA graph holding 20 launches (after 3 warm-up
+    launches), and the error against FP64 on sampled rows."""
     import torch
     import bfly
     import oracle.fft_oracle as O
@@ -293,16 +295,24 @@ def extra_measurements(dev, stream):
     peak, _ = load_peaks()
 
     def timed(fn, reps=20):
+        # warm-up outside the capture (table builds, workspaces), then `reps` launches captured
+        # in one CUDA graph and replayed: the figure is device time, not Python call rate
         for _ in range(3):
             fn()
         stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            for _ in range(reps):
+                fn()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            fn()
-        e1.record(stream)
+        with torch.cuda.stream(stream):
+            graph.replay()
+            e0.record(stream)
+            graph.replay()
+            e1.record(stream)
         e1.synchronize()
+        del graph
         return e0.elapsed_time(e1) / reps
 
     def rel(y, x, inverse=False, rows=4):
@@ -345,7 +355,7 @@ def extra_measurements(dev, stream):
             "fwd_gbs": round(byts / (ms_f / 1e3) / 1e9, 1), "bwd_gbs": round(byts / (ms_b / 1e3) / 1e9, 1),
             "fwd_bwd_gbs": round(2 * byts / ((ms_f + ms_b) / 1e3) / 1e9, 1),
             "fwd_rel_l2": rel(y, x, rows=2), "bwd_rel_l2": rel(z, y, inverse=True, rows=2),
-            "schedule": "single pass" if n <= 8192 else "four-step (2 HBM passes)"}
+            "schedule": "single pass" if n <= 16384 else "four-step (2 HBM passes)"}
         del x, y, z
     # ---- real transforms: R2C forward and its adjoint (weighted C2R), batch 1024
     for n in (128, 1024, 4096, 8192):
