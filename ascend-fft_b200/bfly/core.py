@@ -147,6 +147,18 @@ class Plan:
         return self._lib.bfly_plan_exec_c2c_async(self._h, d_in, d_out, n, batch, direction,
                                                   scale, stream or None)
 
+    def exec_c2c_2d(self, d_in: int, d_out: int, ny: int, nx: int, batch: int, direction: int = -1,
+                    scale: float = 1.0, stream: int = 0) -> int:
+        """2-D C2C over [batch][ny][nx] complex64 device memory."""
+        return self._lib.bfly_plan_exec_c2c_2d_async(self._h, d_in, d_out, ny, nx, batch, direction,
+                                                     scale, stream or None)
+
+    def exec_c2c_axis(self, d_in: int, d_out: int, n: int, outer: int, inner: int,
+                      direction: int = -1, scale: float = 1.0, stream: int = 0) -> int:
+        """C2C along the middle axis of a contiguous [outer][n][inner] complex64 array."""
+        return self._lib.bfly_plan_exec_c2c_axis_async(self._h, d_in, d_out, n, outer, inner,
+                                                       direction, scale, stream or None)
+
     def exec_r2c(self, d_in: int, d_out: int, n: int, batch: int, s_edge: float = 1.0,
                  s_int: float = 1.0, stream: int = 0) -> int:
         return self._lib.bfly_plan_exec_r2c_async(self._h, d_in, d_out, n, batch, s_edge, s_int,

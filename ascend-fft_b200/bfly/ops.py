@@ -1,13 +1,16 @@
 """torch.fft-style functions on CUDA tensors backed by the hand-written sm_100a kernels, with
 hand-written adjoints behind torch.autograd.Function:
 
-    fft(x)   / ifft(x)      complex64 [..., n], n in 32..65536 (four-step above 16384 points
-                            per row, or when the plan schedules it)
+    fft(x, dim) / ifft(x, dim)  complex64, n in 32..65536 along the last dim (four-step above
+                            16384 points per row), 32..4096 along any other dim (column kernel
+                            over the contiguous [outer][n][inner] view)
+    fft2(x) / ifft2(x)      complex64 [..., ny, nx]: row pass (nx as fft) + column pass
+                            (ny in 32..4096)
     rfft(x)                 float32 [..., n] -> complex64 [..., n/2+1], n in 64..8192
     irfft(X, n)             complex64 [..., n/2+1] -> float32 [..., n]
 
 `norm` follows torch.fft ("backward", "ortho", "forward").  Adjoints:
-    fft  : grad_x = s * IFFT_unnormalised(g)          (conjugate FFT)
+    fft  : grad_x = s * IFFT_unnormalised(g)          (conjugate FFT; same for fft2 and any dim)
     ifft : grad_x = s * FFT(g)
     rfft : grad_x = C2R(g) with bins 0 and n/2 weighted 1 and the others 1/2, times s
     irfft: grad_X = R2C(g) with bins 0 and n/2 weighted c and the others 2c  (c = output scale)
@@ -163,6 +166,74 @@ def c2r(X: torch.Tensor, n: int, s_edge: float = 1.0, s_int: float = 1.0,
     return y
 
 
+def _outer_inner(shape, dim: int):
+    outer = 1
+    for s in shape[:dim]:
+        outer *= s
+    inner = 1
+    for s in shape[dim + 1:]:
+        inner *= s
+    return outer, inner
+
+
+def c2c_axis(x: torch.Tensor, dim: int, direction: int, scale: float) -> torch.Tensor:
+    """C2C along dimension `dim` of a complex64 CUDA tensor (any dim; contiguous copy made)."""
+    _need_cuda(x, torch.complex64, "c2c_axis")
+    dim = dim % x.dim()
+    if dim == x.dim() - 1:
+        return c2c(x, direction, scale)
+    x = x.contiguous()
+    n = x.shape[dim]
+    outer, inner = _outer_inner(x.shape, dim)
+    y = torch.empty_like(x)
+    if x.numel() == 0:
+        return y
+    rc = plan_for(x.device, n).exec_c2c_axis(x.data_ptr(), y.data_ptr(), n, outer, inner, direction, scale,
+                                             _stream(x))
+    if rc:
+        raise BflyError(f"exec_c2c_axis(n={n}, outer={outer}, inner={inner})", rc)
+    return y
+
+
+def c2c_2d(x: torch.Tensor, direction: int, scale: float) -> torch.Tensor:
+    """2-D C2C over the last two dimensions of a complex64 CUDA tensor."""
+    _need_cuda(x, torch.complex64, "c2c_2d")
+    _need_2d(x, "c2c_2d")
+    x = x.contiguous()
+    ny, nx = x.shape[-2], x.shape[-1]
+    batch = x.numel() // (ny * nx) if ny * nx else 0
+    y = torch.empty_like(x)
+    if batch == 0:
+        return y
+    rc = plan_for(x.device, nx).exec_c2c_2d(x.data_ptr(), y.data_ptr(), ny, nx, batch, direction, scale,
+                                            _stream(x))
+    if rc:
+        raise BflyError(f"exec_c2c_2d(ny={ny}, nx={nx}, batch={batch})", rc)
+    return y
+
+
+class _FFTAxis(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, dim, direction, scale):
+        ctx.dim, ctx.direction, ctx.scale = dim, direction, scale
+        return c2c_axis(x, dim, direction, scale)
+
+    @staticmethod
+    def backward(ctx, g):
+        return c2c_axis(g, ctx.dim, -ctx.direction, ctx.scale), None, None, None
+
+
+class _FFT2(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, direction, scale):
+        ctx.direction, ctx.scale = direction, scale
+        return c2c_2d(x, direction, scale)
+
+    @staticmethod
+    def backward(ctx, g):
+        return c2c_2d(g, -ctx.direction, ctx.scale), None, None
+
+
 class _FFT(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, direction, scale):
@@ -213,12 +284,32 @@ def c2c_tensor(x: torch.Tensor, direction: int = -1, scale: float = 1.0, split_t
     return y
 
 
-def fft(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:
+def fft(x: torch.Tensor, norm: str | None = None, dim: int = -1) -> torch.Tensor:
+    if dim % max(x.dim(), 1) != x.dim() - 1:
+        return _FFTAxis.apply(x, dim, -1, _scale(norm, x.shape[dim], True))
     return _FFT.apply(x, -1, _scale(norm, x.shape[-1], True))
 
 
-def ifft(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:
+def ifft(x: torch.Tensor, norm: str | None = None, dim: int = -1) -> torch.Tensor:
+    if dim % max(x.dim(), 1) != x.dim() - 1:
+        return _FFTAxis.apply(x, dim, 1, _scale(norm, x.shape[dim], False))
     return _FFT.apply(x, 1, _scale(norm, x.shape[-1], False))
+
+
+def _need_2d(x: torch.Tensor, what: str):
+    if x.dim() < 2:
+        raise ValueError(f"{what}: input needs at least two dimensions")
+
+
+def fft2(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:
+    """2-D FFT over the last two dimensions (torch.fft.fft2 with dim=(-2, -1))."""
+    _need_2d(x, "fft2")
+    return _FFT2.apply(x, -1, _scale(norm, x.shape[-2] * x.shape[-1], True))
+
+
+def ifft2(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:
+    _need_2d(x, "ifft2")
+    return _FFT2.apply(x, 1, _scale(norm, x.shape[-2] * x.shape[-1], False))
 
 
 def rfft(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:

@@ -75,6 +75,13 @@ int launchLongCluster(const void* in, void* out, uint32_t n, uint64_t batch, boo
                       const void* tw1, const void* tw2, const void* tlo, const void* thi, int cta, void* stream);
 int longClusterStatus(unsigned* status, bool clear);   // device error word of the cluster kernel; 0 on success
 
+// Column FFTs: ny-point transforms down the ncols columns of `mats` row-major matrices,
+// element (m, i, col) at m*matStride + i*pitch + col (float2 units).  ny in 32..4096;
+// tw = Stockham table (ny, 16); in == out allowed.
+bool hasCols(uint32_t ny);
+int launchCols(const void* in, void* out, uint32_t ny, uint32_t ncols, uint64_t pitch, uint64_t matStride,
+               uint64_t mats, bool inverse, float scale, const void* tw, void* stream);
+
 // Ragged persistent launch over a device array of RaggedEntry (ragged.h).
 int raggedSmemBytes();
 int raggedGrid(int device, int* grid);   // resident CTAs on the whole device

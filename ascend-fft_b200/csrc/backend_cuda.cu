@@ -7,6 +7,7 @@
 #include <atomic>
 #include <cstring>
 #include <mutex>
+#include <utility>
 
 namespace bfly {
 namespace backend {
@@ -92,16 +93,19 @@ size_t variantSmemBytes(int kind, uint32_t n, int e, int cta) {
 }
 
 // Raise the dynamic shared-memory limit once per kernel that needs more than 48 KB.
+// Opt a kernel into more than 48 KB of dynamic shared memory, once per (device, kernel).
 static int prepareEntry(const Entry* x) {
     if (x->smem <= 48 * 1024) return 0;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return (int)cudaErrorInvalidDevice;
     static std::mutex mu;
-    static const Entry* done[512];
+    static std::pair<int, const Entry*> done[1024];
     static int ndone = 0;
     std::lock_guard<std::mutex> lock(mu);
     for (int i = 0; i < ndone; ++i)
-        if (done[i] == x) return 0;
+        if (done[i].first == device && done[i].second == x) return 0;
     int e = rc(cudaFuncSetAttribute(x->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, x->smem));
-    if (!e && ndone < 512) done[ndone++] = x;
+    if (!e && ndone < 1024) done[ndone++] = {device, x};
     return e;
 }
 
@@ -197,6 +201,23 @@ int launchLongA(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
     fn<<<(unsigned)grid, x->cta, x->smem, S(stream)>>>(
         static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw1),
         static_cast<const float2*>(tlo), static_cast<const float2*>(thi), batch, ilog2u(n2));
+    return rc(cudaGetLastError());
+}
+
+bool hasCols(uint32_t ny) { return dev::findCols(ny, false) != nullptr; }
+
+int launchCols(const void* in, void* out, uint32_t ny, uint32_t ncols, uint64_t pitch, uint64_t matStride,
+               uint64_t mats, bool inverse, float scale, const void* tw, void* stream) {
+    const Entry* x = dev::findCols(ny, inverse);
+    if (!x || ncols == 0 || mats == 0) return (int)cudaErrorInvalidValue;
+    const uint32_t colBlocks = (ncols + (uint32_t)x->rows - 1) / (uint32_t)x->rows;
+    const uint64_t grid = mats * colBlocks;
+    if (grid > 0x7fffffffull) return (int)cudaErrorInvalidValue;
+    if (int err = prepareEntry(x)) return err;
+    auto fn = reinterpret_cast<dev::KCols>(const_cast<void*>(x->fn));
+    fn<<<(unsigned)grid, x->cta, x->smem, S(stream)>>>(static_cast<const float2*>(in), static_cast<float2*>(out),
+                                                      static_cast<const float2*>(tw), ncols, pitch, matStride,
+                                                      colBlocks, scale);
     return rc(cudaGetLastError());
 }
 

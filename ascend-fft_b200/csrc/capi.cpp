@@ -167,6 +167,19 @@ int bfly_plan_exec_c2c_async(bfly_plan* plan, const void* d_in, void* d_out, uin
     return p.execC2C(d_in, d_out, n, batch, direction, scale, stream);
 }
 
+int bfly_plan_exec_c2c_2d_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t ny,
+                                uint32_t nx, uint64_t batch, int direction, float scale, void* stream) {
+    PLAN_OR_FAIL();
+    return p.execC2C2D(d_in, d_out, ny, nx, batch, direction, scale, stream);
+}
+
+int bfly_plan_exec_c2c_axis_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
+                                  uint64_t outer, uint64_t inner, int direction, float scale,
+                                  void* stream) {
+    PLAN_OR_FAIL();
+    return p.execC2CAxis(d_in, d_out, n, outer, inner, direction, scale, stream);
+}
+
 int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, float s_edge, float s_int, void* stream) {
     PLAN_OR_FAIL();

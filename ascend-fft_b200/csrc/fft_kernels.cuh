@@ -150,6 +150,37 @@ k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     if (ok) TM::for_each_out(v, t, [&](int i, float2 x) { st_stream(dst + i, x); });
 }
 
+// ------------------------------------------------------------------ column FFTs
+// NY-point FFTs down the columns of a batch of row-major matrices:
+//   in[m*matStride + i*pitch + col], i < NY, col < ncols, m < gridDim.x / colBlocks.
+// Serves the column pass of a 2-D transform ([batch][ny][nx]: pitch = nx, matStride = ny*nx)
+// and transforms along a middle axis of a contiguous [outer][n][inner] array (pitch = inner).
+// C consecutive columns per CTA with the column index fastest across threads, so every row
+// access is one C*8-byte segment; columns at or past ncols compute on zeros and store nothing.
+// Every load precedes the CTA's first __syncthreads and every store follows its last, so
+// in == out is allowed.
+template <int NY, int E, int C, bool INV>
+__global__ void __launch_bounds__((NY / E) * C, min_blocks_64regs((NY / E) * C))
+k_cols(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
+       uint32_t ncols, uint64_t pitch, uint64_t matStride, uint32_t colBlocks, float scale) {
+    constexpr int S = smem_stride<NY, E, true>();
+    using TM = Team<NY, E, INV, kSyncBlock>;
+    static_assert(TM::P >= 2, "in-place safety needs a barrier between loads and stores");
+    extern __shared__ float2 smem[];
+    const int c = threadIdx.x % C;
+    const int t = threadIdx.x / C;
+    const uint64_t m = blockIdx.x / colBlocks;
+    const uint32_t col = (blockIdx.x % colBlocks) * C + c;
+    const bool live = col < ncols;
+    const float2* src = in + m * matStride + (live ? col : 0u);
+    float2* dst = out + m * matStride + col;
+    float2 v[E];
+    TM::run(v, smem + c * S, tw, t, 0, [&](int i) {
+        return live ? ld_stream(src + (size_t)i * pitch) : make_float2(0.f, 0.f);
+    });
+    if (live) TM::for_each_out(v, t, [&](int k, float2 x) { st_stream(dst + (size_t)k * pitch, cscale(x, scale)); });
+}
+
 // ------------------------------------------------------------------ four-step long C2C
 // x[b][N2*n1 + n2] -> (pass A) y[b][N2*k1 + n2] = W_N^(n2*k1) * FFT_N1 over n1
 //                  -> (pass B) X[b][k1 + N1*k2]  = FFT_N2 over n2 of y[b][N2*k1 + :]

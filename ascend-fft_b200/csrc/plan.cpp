@@ -525,7 +525,7 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
     void* s = stream;   // NULL is the CUDA default stream
     const bool inv = direction > 0;
     int e = 0, cta = 0;
-    resolve(backend::kC2C, n, &e, &cta);
+    if (resolve(backend::kC2C, n, &e, &cta)) return -1;
     if (e > 0) {
         if (prepareC2C(n, e)) return -2;
         if (backend::launchC2C(dIn, dOut, n, batch, inv, scale, impl_->twC2C[{n, e}], e, cta, s)) return -5;
@@ -588,12 +588,42 @@ int Plan::longStatus(unsigned* status) {
     return backend::longClusterStatus(status, true) ? -6 : 0;
 }
 
+// Column pass shared by the 2-D and axis entry points: n-point transforms down `cols`
+// columns of `mats` matrices with row pitch `pitch`.
+int Plan::execCols(const void* dIn, void* dOut, uint32_t n, uint64_t mats, uint32_t cols,
+                   uint64_t pitch, bool inverse, float scale, void* stream) {
+    if (!backend::hasCols(n)) return -8;
+    if (prepareC2C(n, kColsE)) return -2;
+    if (backend::launchCols(dIn, dOut, n, cols, pitch, (uint64_t)n * pitch, mats, inverse, scale,
+                            impl_->twC2C[{n, kColsE}], stream))
+        return -5;
+    return 0;
+}
+
+int Plan::execC2C2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch,
+                    int direction, float scale, void* stream) {
+    if (!dIn || !dOut || batch == 0 || (direction != -1 && direction != 1)) return -8;
+    if (!pow2(ny) || !backend::hasCols(ny)) return -8;
+    if (batch * ny > 0xFFFFFFFFull || !validShape(nx, (uint32_t)(batch * ny), kExecC2C)) return -8;
+    if (int r = execC2CWith(dIn, dOut, nx, batch * ny, direction, 1.0f, stream, nullptr)) return r;
+    return execCols(dOut, dOut, ny, batch, nx, nx, direction > 0, scale, stream);
+}
+
+int Plan::execC2CAxis(const void* dIn, void* dOut, uint32_t n, uint64_t outer, uint64_t inner,
+                      int direction, float scale, void* stream) {
+    if (!dIn || !dOut || outer == 0 || inner == 0 || (direction != -1 && direction != 1)) return -8;
+    if (inner == 1) return execC2C(dIn, dOut, n, outer, direction, scale, stream);
+    if (!pow2(n) || !backend::hasCols(n) || inner > 0xFFFFFFFFull) return -8;
+    if (outer > (~0ull) / n / inner) return -8;
+    return execCols(dIn, dOut, n, outer, (uint32_t)inner, inner, direction > 0, scale, stream);
+}
+
 int Plan::execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
                   float sInt, void* stream) {
     if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull) return -8;
     if (!validShape(n, (uint32_t)batch, kExecR2C)) return -8;
     int e = 0, cta = 0;
-    resolve(backend::kR2C, n, &e, &cta);
+    if (resolve(backend::kR2C, n, &e, &cta)) return -1;
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
     const bool weighted = !(sEdge == 1.0f && sInt == 1.0f);
     if (backend::launchR2C(dIn, dOut, n, batch, impl_->twC2C[{n / 2, e}], impl_->twReal[n], e, cta,
@@ -607,7 +637,7 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
     if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull) return -8;
     if (!validShape(n, (uint32_t)batch, kExecC2R)) return -8;
     int e = 0, cta = 0;
-    resolve(backend::kC2R, n, &e, &cta);
+    if (resolve(backend::kC2R, n, &e, &cta)) return -1;
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
     if (backend::launchC2R(dIn, dOut, n, batch, impl_->twC2C[{n / 2, e}], impl_->twReal[n], e, cta,
                            sEdge, sInt, outScale, stream))
@@ -687,7 +717,7 @@ int Plan::runLong(const float* in, float* out, uint32_t n, uint32_t batch, int d
     if (!in || !out || (direction != -1 && direction != 1) || !validShape(n, batch, kRunLong)) return -8;
     if (prepare(n, batch)) return -2;
     int e = 0, cta = 0;
-    resolve(backend::kC2C, n, &e, &cta);
+    if (resolve(backend::kC2C, n, &e, &cta)) return -1;
     if (e == 0 && ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
     // chunks on different streams use disjoint slices of the four-step workspace
     return roundTrip(in, (size_t)n * 8, out, (size_t)n * 8, batch,
@@ -700,7 +730,7 @@ int Plan::runLong(const float* in, float* out, uint32_t n, uint32_t batch, int d
 int Plan::runR2C(const float* in, float* out, uint32_t n, uint32_t batch) {
     if (!in || !out || !validShape(n, batch, kRunR2C)) return -8;
     int e = 0, cta = 0;
-    resolve(backend::kR2C, n, &e, &cta);
+    if (resolve(backend::kR2C, n, &e, &cta)) return -1;
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
     return roundTrip(in, (size_t)n * 4, out, (size_t)(n + 2) * 4, batch,
                      [&](void* di, void* dout, uint32_t, uint32_t rows, void* st) {
@@ -711,7 +741,7 @@ int Plan::runR2C(const float* in, float* out, uint32_t n, uint32_t batch) {
 int Plan::runC2R(const float* in, float* out, uint32_t n, uint32_t batch) {
     if (!in || !out || !validShape(n, batch, kRunC2R)) return -8;
     int e = 0, cta = 0;
-    resolve(backend::kC2R, n, &e, &cta);
+    if (resolve(backend::kC2R, n, &e, &cta)) return -1;
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
     return roundTrip(in, (size_t)(n + 2) * 4, out, (size_t)n * 4, batch,
                      [&](void* di, void* dout, uint32_t, uint32_t rows, void* st) {

@@ -15,6 +15,7 @@ using KC2R = void (*)(const float2*, float2*, const float2*, const float2*, uint
 using KLongA = void (*)(const float2*, float2*, const float2*, const float2*, const float2*,
                         uint64_t, int);
 using KLongB = void (*)(const float2*, float2*, const float2*, uint64_t, int, float);
+using KCols = void (*)(const float2*, float2*, const float2*, uint32_t, uint64_t, uint64_t, uint32_t, float);
 using KTw = void (*)(float2*);
 
 struct Entry {
@@ -34,6 +35,7 @@ const Entry* findR2C(uint32_t n, int e, int cta, bool weighted);
 const Entry* findC2R(uint32_t n, int e, int cta);
 const Entry* findLongA(uint32_t n1, bool inverse);
 const Entry* findLongB(uint32_t n2, bool inverse);
+const Entry* findCols(uint32_t ny, bool inverse);   // rows = columns per CTA
 // Stockham twiddle builder for Sched<n,e> and its table size.
 bool findTw(uint32_t n, int e, KTw* fn, int* count);
 

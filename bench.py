@@ -284,8 +284,8 @@ def run_reference(args):
 def extra_measurements(dev, stream):
     """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores vs fp32 at the
     largest power-of-16 grid points; long C2C forward + backward (batch*n = 2^26; single pass up
-    to n = 16384, four-step above);
-    real transforms forward + adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
+    to n = 16384, four-step above); 2-D C2C at the reference's planned 2-D / range-Doppler shapes
+    and transforms along a middle axis; real transforms forward + adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
     events on `stream` around one replay of a CUDA graph holding 20 launches (after 3 warm-up
     launches), and the error against FP64 on sampled rows."""
     import torch
@@ -357,6 +357,36 @@ def extra_measurements(dev, stream):
             "fwd_rel_l2": rel(y, x, rows=2), "bwd_rel_l2": rel(z, y, inverse=True, rows=2),
             "schedule": "single pass" if n <= 16384 else "four-step (2 HBM passes)"}
         del x, y, z
+    # ---- 2-D C2C (row pass + column pass) at the reference's planned 2-D / range-Doppler
+    # shapes, batch * ny * nx = 2^26; and transforms along the middle axis of [outer][n][inner]
+    out["c2c_2d"] = {}
+    for ny, nx in ((256, 256), (512, 512), (1024, 1024), (2048, 2048), (1024, 128), (128, 1024)):
+        b = (1 << 26) // (ny * nx)
+        g = torch.Generator(device=dev).manual_seed(ny + nx)
+        x = torch.randn(b, ny, nx, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.empty_like(x)
+        plan = bfly.plan_for(dev, nx)
+        ms = timed(lambda: plan.exec_c2c_2d(x.data_ptr(), y.data_ptr(), ny, nx, b, -1, 1.0, sh))
+        xs = x[:1].cpu().numpy().astype(np.complex128)
+        ref = np.fft.fft2(xs).reshape(1, -1)
+        err = float(np.linalg.norm(y[:1].cpu().numpy().reshape(1, -1) - ref) / np.linalg.norm(ref))
+        out["c2c_2d"][f"{ny}x{nx}_b{b}"] = {"gbs": round(16 * ny * nx * b / ms / 1e6, 1),
+                                           "frac": round(16 * ny * nx * b / ms / 1e6 / peak, 4),
+                                           "rel_l2": err, "passes": 2}
+        del x, y
+    for n, outer, inner in ((1024, 64, 1024), (256, 1024, 256)):
+        g = torch.Generator(device=dev).manual_seed(n + inner)
+        x = torch.randn(outer, n, inner, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.empty_like(x)
+        plan = bfly.plan_for(dev, n)
+        ms = timed(lambda: plan.exec_c2c_axis(x.data_ptr(), y.data_ptr(), n, outer, inner, -1, 1.0, sh))
+        xs = x[:1].cpu().numpy().astype(np.complex128)
+        ref = np.fft.fft(xs, axis=1)
+        err = float(np.linalg.norm(y[:1].cpu().numpy() - ref) / np.linalg.norm(ref))
+        out["c2c_2d"][f"axis_n{n}_outer{outer}_inner{inner}"] = {
+            "gbs": round(16 * n * outer * inner / ms / 1e6, 1),
+            "frac": round(16 * n * outer * inner / ms / 1e6 / peak, 4), "rel_l2": err, "passes": 1}
+        del x, y
     # ---- real transforms: R2C forward and its adjoint (weighted C2R), batch 1024
     for n in (128, 1024, 4096, 8192):
         b = 1024

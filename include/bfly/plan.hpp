@@ -190,6 +190,16 @@ public:
     //   n in [32, 16384] single pass, [8192, 65536] four-step (workspace grown on demand).
     int execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                 float scale, void* stream);
+    // 2-D C2C over [batch][ny][nx] complex, rows of nx contiguous: nx-point row transforms
+    // (any execC2C length) into dOut, then ny-point column transforms in place in dOut
+    // (ny in [32, 4096]); scale applied once.  batch * ny <= 2^32 - 1.
+    int execC2C2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch,
+                  int direction, float scale, void* stream);
+    // C2C along the middle axis of a contiguous [outer][n][inner] complex array: element i of
+    // transform (o, c) at (o*n + i)*inner + c.  inner == 1 is execC2C (n in [32, 65536]);
+    // inner > 1 runs the column kernel (n in [32, 4096]).  dIn == dOut allowed.
+    int execC2CAxis(const void* dIn, void* dOut, uint32_t n, uint64_t outer, uint64_t inner,
+                    int direction, float scale, void* stream);
     // R2C [batch][n] -> [batch][n/2+1] complex, bins scaled by (sEdge at 0 and n/2, sInt
     // elsewhere); sEdge = sInt = 1 is the plain transform.
     int execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
@@ -225,6 +235,9 @@ private:
     int resolve(int kind, uint32_t n, int* e, int* cta) const;
     int execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                     float scale, void* stream, void* work);
+    static constexpr int kColsE = 16;   // complex values per thread of the column kernels
+    int execCols(const void* dIn, void* dOut, uint32_t n, uint64_t mats, uint32_t cols, uint64_t pitch,
+                 bool inverse, float scale, void* stream);
     // Upload / enqueue / download of host buffers, pipelined over row chunks on several
     // streams for large batches.  enqueue(dIn, dOut, firstRow, rows, stream) -> exec status.
     template <class Enqueue>

@@ -114,6 +114,21 @@ int bfly_plan_run_c2c_long(bfly_plan* plan, const float* in, float* out, uint32_
 /* C2C, n in [32, 65536]; direction -1 forward / +1 inverse; output multiplied by scale. */
 int bfly_plan_exec_c2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, int direction, float scale, void* stream);
+/* New: 2-D C2C over [batch][ny][nx] complex (rows of nx contiguous): nx-point row transforms
+ * (any exec_c2c length) into d_out, then ny-point column transforms in place in d_out,
+ * ny in [32, 4096]; scale applied once; batch * ny <= 2^32 - 1.  The reference has no 2-D
+ * transform (docs/reference/support.md:14; docs/testing.md:20 and :120 plan range-Doppler and
+ * 2-D at 256^2..2048^2 and 1024x128). */
+int bfly_plan_exec_c2c_2d_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t ny,
+                                uint32_t nx, uint64_t batch, int direction, float scale,
+                                void* stream);
+/* New: C2C along the middle axis of a contiguous [outer][n][inner] complex array (element i
+ * of transform (o, c) at (o*n + i)*inner + c): inner == 1 is exec_c2c; inner > 1 needs n in
+ * [32, 4096].  d_in == d_out allowed.  The reference supports contiguous rows only
+ * (docs/reference/support.md:11 and docs/testing.md:21 list strided layouts as missing). */
+int bfly_plan_exec_c2c_axis_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
+                                  uint64_t outer, uint64_t inner, int direction, float scale,
+                                  void* stream);
 /* R2C [batch][n] -> [batch][n/2+1] complex, n in [64, 8192]; bins 0 and n/2 scaled by
  * s_edge, the others by s_int (1, 1 for the plain transform). */
 int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,

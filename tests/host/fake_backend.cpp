@@ -141,6 +141,29 @@ int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
     return 0;
 }
 
+bool hasCols(uint32_t ny) { return ny >= 32 && ny <= 4096 && !(ny & (ny - 1)); }
+int launchCols(const void* in, void* out, uint32_t ny, uint32_t ncols, uint64_t pitch, uint64_t matStride,
+               uint64_t mats, bool inverse, float scale, const void*, void*) {
+    if (!hasCols(ny) || ncols == 0 || mats == 0) return 1;
+    if (int r = launch()) return r;
+    std::vector<float> col(2 * ny), res(2 * ny);   // gather a column, transform, scatter (in == out allowed)
+    for (uint64_t m = 0; m < mats; ++m)
+        for (uint32_t c = 0; c < ncols; ++c) {
+            const float* src = (const float*)in + 2 * (m * matStride + c);
+            float* dst = (float*)out + 2 * (m * matStride + c);
+            for (uint32_t i = 0; i < ny; ++i) {
+                col[2 * i] = src[2 * i * pitch];
+                col[2 * i + 1] = src[2 * i * pitch + 1];
+            }
+            dft(col.data(), res.data(), ny, inverse ? 1 : -1, scale);
+            for (uint32_t i = 0; i < ny; ++i) {
+                dst[2 * i * pitch] = res[2 * i];
+                dst[2 * i * pitch + 1] = res[2 * i + 1];
+            }
+        }
+    return 0;
+}
+
 bool hasLongCluster(uint32_t n, int cta) {
     return (n == 8192 && cta == 256) || ((n == 16384 || n == 32768 || n == 65536) && (cta == 256 || cta == 512));
 }

@@ -6,6 +6,7 @@
 // select acceptance, and the persisted tuning cache.
 #include "bfly/plan.hpp"
 
+#include <algorithm>
 #include <cassert>
 #include <cmath>
 #include <cstdio>
@@ -357,6 +358,87 @@ int main(int argc, char** argv) {
         fake::failAllocation = fake::allocations + 1;
         CHECK(!plan->makeRagged(ok, 2, &st) && st == -3);
         fake::failAllocation = 0;
+    }
+
+    {   // 2-D and middle-axis transforms: exact against a direct FP64 DFT of the same layout
+        auto dft2 = [](const std::vector<float>& x, uint32_t ny, uint32_t nx, uint32_t batch, int sign) {
+            std::vector<double> y(x.size());
+            for (uint32_t b = 0; b < batch; ++b)
+                for (uint32_t ky = 0; ky < ny; ++ky)
+                    for (uint32_t kx = 0; kx < nx; ++kx) {
+                        double re = 0, im = 0;
+                        for (uint32_t iy = 0; iy < ny; ++iy)
+                            for (uint32_t ix = 0; ix < nx; ++ix) {
+                                const double a = sign * 2 * M_PI *
+                                                 ((double)((iy * ky) % ny) / ny + (double)((ix * kx) % nx) / nx);
+                                const size_t at = 2 * (((size_t)b * ny + iy) * nx + ix);
+                                re += x[at] * std::cos(a) - x[at + 1] * std::sin(a);
+                                im += x[at] * std::sin(a) + x[at + 1] * std::cos(a);
+                            }
+                        const size_t o = 2 * (((size_t)b * ny + ky) * nx + kx);
+                        y[o] = re;
+                        y[o + 1] = im;
+                    }
+            return y;
+        };
+        auto maxErr = [](const std::vector<float>& got, const std::vector<double>& ref, double scale) {
+            double e = 0, m = 0;
+            for (size_t i = 0; i < got.size(); ++i) {
+                e = std::max(e, std::fabs(got[i] - ref[i] * scale));
+                m = std::max(m, std::fabs(ref[i] * scale));
+            }
+            return e / std::max(1.0, m);
+        };
+        const uint32_t ny = 32, nx = 64, batch = 2;
+        std::vector<float> x(2 * ny * nx * batch), y(x.size());
+        for (size_t i = 0; i < x.size(); ++i) x[i] = (float)std::sin(0.37 * i + 0.1 * (i % 7));
+        CHECK(plan->execC2C2D(x.data(), y.data(), ny, nx, batch, -1, 1.f, nullptr) == 0);
+        CHECK(maxErr(y, dft2(x, ny, nx, batch, -1), 1.0) < 1e-5);
+        CHECK(plan->execC2C2D(x.data(), y.data(), ny, nx, batch, 1, 0.25f, nullptr) == 0);
+        CHECK(maxErr(y, dft2(x, ny, nx, batch, 1), 0.25) < 1e-5);
+        // middle axis of [outer][n][inner]: the same data read as [2][32][64] transformed along
+        // the 32-point axis equals the column pass of the 2-D transform alone
+        std::vector<float> axis(x.size());
+        CHECK(plan->execC2CAxis(x.data(), axis.data(), 32, 2, 64, -1, 1.f, nullptr) == 0);
+        double e = 0;
+        for (uint32_t b = 0; b < 2; ++b)
+            for (uint32_t c = 0; c < 64; ++c)
+                for (uint32_t k = 0; k < 32; ++k) {
+                    double re = 0, im = 0;
+                    for (uint32_t i = 0; i < 32; ++i) {
+                        const double a = -2 * M_PI * (double)((i * k) % 32) / 32;
+                        const size_t at = 2 * (((size_t)b * 32 + i) * 64 + c);
+                        re += x[at] * std::cos(a) - x[at + 1] * std::sin(a);
+                        im += x[at] * std::sin(a) + x[at + 1] * std::cos(a);
+                    }
+                    const size_t o = 2 * (((size_t)b * 32 + k) * 64 + c);
+                    e = std::max(e, std::max(std::fabs(axis[o] - re), std::fabs(axis[o + 1] - im)));
+                }
+        CHECK(e < 1e-3);
+        // in place, and inner == 1 is the plain row transform
+        std::vector<float> inplace = x;
+        CHECK(plan->execC2CAxis(inplace.data(), inplace.data(), 32, 2, 64, -1, 1.f, nullptr) == 0);
+        CHECK(inplace == axis);
+        std::vector<float> rows1(x.size()), rows2(x.size());
+        CHECK(plan->execC2CAxis(x.data(), rows1.data(), 64, 64, 1, -1, 1.f, nullptr) == 0);
+        CHECK(plan->execC2C(x.data(), rows2.data(), 64, 64, -1, 1.f, nullptr) == 0);
+        CHECK(rows1 == rows2);
+        // guards: -8 before any allocation or launch
+        const int allocBefore = fake::allocations, launchBefore = fake::launches;
+        float* d = x.data();
+        CHECK(plan->execC2C2D(nullptr, d, 32, 64, 1, -1, 1.f, nullptr) == -8);
+        CHECK(plan->execC2C2D(d, d, 32, 64, 0, -1, 1.f, nullptr) == -8);
+        CHECK(plan->execC2C2D(d, d, 32, 64, 1, 2, 1.f, nullptr) == -8);
+        CHECK(plan->execC2C2D(d, d, 16, 64, 1, -1, 1.f, nullptr) == -8);      // ny below 32
+        CHECK(plan->execC2C2D(d, d, 8192, 64, 1, -1, 1.f, nullptr) == -8);    // ny above 4096
+        CHECK(plan->execC2C2D(d, d, 48, 64, 1, -1, 1.f, nullptr) == -8);      // ny not a power of two
+        CHECK(plan->execC2C2D(d, d, 32, 96, 1, -1, 1.f, nullptr) == -8);      // nx not a power of two
+        CHECK(plan->execC2C2D(d, d, 4096, 64, 1u << 20, -1, 1.f, nullptr) == -8);   // batch*ny > 2^32-1
+        CHECK(plan->execC2CAxis(d, d, 32, 0, 3, -1, 1.f, nullptr) == -8);
+        CHECK(plan->execC2CAxis(d, d, 32, 1, 0, -1, 1.f, nullptr) == -8);
+        CHECK(plan->execC2CAxis(d, d, 8192, 1, 3, -1, 1.f, nullptr) == -8);   // strided n above 4096
+        CHECK(plan->execC2CAxis(d, d, 100, 1, 3, -1, 1.f, nullptr) == -8);
+        CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
     }
 
     plan.reset();
