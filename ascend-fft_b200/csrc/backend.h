@@ -75,6 +75,15 @@ int launchLongCluster(const void* in, void* out, uint32_t n, uint64_t batch, boo
                       const void* tw1, const void* tw2, const void* tlo, const void* thi, int cta, void* stream);
 int longClusterStatus(unsigned* status, bool clear);   // device error word of the cluster kernel; 0 on success
 
+// Any-length C2C (Bluestein), n in [2, kBluesteinMaxN], in one kernel per padded length M =
+// bluesteinM(n) (power of two >= 2n-1, >= 64).  Tables per n: chirp (n float2), filter (M
+// float2), built in FP64 on the device with an M-double2 scratch; tw = Stockham table (M, 16).
+constexpr uint32_t kBluesteinMaxN = 8192;
+uint32_t bluesteinM(uint32_t n);   // 0 when n is outside [2, kBluesteinMaxN]
+int buildBluesteinTables(void* chirp, void* filt, void* scratch, uint32_t n, void* stream);
+int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+                    const void* tw, const void* chirp, const void* filt, void* stream);
+
 // Column FFTs: ny-point transforms down the ncols columns of `mats` row-major matrices,
 // element (m, i, col) at m*matStride + i*pitch + col (float2 units).  ny in 32..4096;
 // tw = Stockham table (ny, 16); in == out allowed.

@@ -350,6 +350,11 @@ struct Plan::Impl {
     backend::Timer* timer = nullptr;
     void* aux[2] = {nullptr, nullptr};   // extra streams of the pipelined host round trip
     void* tcTable[4] = {nullptr, nullptr, nullptr, nullptr};   // split DFT-16 operand per term count
+    struct Chirp {
+        void* chirp = nullptr;   // c[j] = exp(-i*pi*j^2/n), j < n
+        void* filt = nullptr;    // FFT_M of the padded conj(c) sequence, / M
+    };
+    std::map<uint32_t, Chirp> bluestein;   // non-power-of-two n -> Bluestein tables
 };
 
 Plan::Plan(Candidate c) : cand_(std::move(c)) {}
@@ -370,6 +375,10 @@ Plan::~Plan() {
         if (st) backend::streamDestroy(st);
     for (void* t : impl_->tcTable)
         if (t) backend::release(t);
+    for (auto& kv : impl_->bluestein) {
+        if (kv.second.chirp) backend::release(kv.second.chirp);
+        if (kv.second.filt) backend::release(kv.second.filt);
+    }
 }
 
 static int ensureBuf(void** p, size_t* cap, size_t bytes) {
@@ -388,7 +397,10 @@ static int ensureBuf(void** p, size_t* cap, size_t bytes) {
 }
 
 bool Plan::validShape(uint32_t n, uint32_t batch, int kind) const {
-    if (!impl_ || batch == 0 || !pow2(n)) return false;
+    if (!impl_ || batch == 0) return false;
+    // lengths outside the power-of-two kernels (non-powers of two, and 2..16) only through the
+    // device-pointer C2C entry (Bluestein)
+    if (!pow2(n) || (kind == kExecC2C && n < kMinN)) return kind == kExecC2C && backend::bluesteinM(n) != 0;
     const bool offsetGuard = kind == kRunC2C || kind == kRunR2C || kind == kRunC2R ||
                              kind == kRunLong || kind == kMeasure;
     switch (kind) {
@@ -497,6 +509,30 @@ int Plan::prepareLong(uint32_t n) {
     return 0;
 }
 
+int Plan::prepareBluestein(uint32_t n) {
+    const uint32_t M = backend::bluesteinM(n);
+    if (!M || prepareC2C(M, kColsE)) return -1;
+    if (impl_->bluestein.count(n)) return 0;
+    Impl::Chirp t;
+    void* scratch = nullptr;
+    if (backend::alloc(&t.chirp, (size_t)n * 8) || backend::alloc(&t.filt, (size_t)M * 8) ||
+        backend::alloc(&scratch, (size_t)M * 16)) {
+        if (t.chirp) backend::release(t.chirp);
+        if (t.filt) backend::release(t.filt);
+        return -1;
+    }
+    const bool bad = backend::buildBluesteinTables(t.chirp, t.filt, scratch, n, stream_) ||
+                     backend::streamSync(stream_);
+    backend::release(scratch);
+    if (bad) {
+        backend::release(t.chirp);
+        backend::release(t.filt);
+        return -1;
+    }
+    impl_->bluestein[n] = t;
+    return 0;
+}
+
 int Plan::prepare(uint32_t n, uint32_t batch) {
     if (!validShape(n, batch, kPrepare)) return -8;
     int e = 0, cta = 0;
@@ -524,6 +560,14 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
     if (!validShape(n, (uint32_t)batch, kExecC2C)) return -8;
     void* s = stream;   // NULL is the CUDA default stream
     const bool inv = direction > 0;
+    if (!pow2(n) || n < kMinN) {   // Bluestein: one kernel on the padded power-of-two length
+        if (prepareBluestein(n)) return -2;
+        const auto& t = impl_->bluestein[n];
+        if (backend::launchBluestein(dIn, dOut, n, batch, inv, scale,
+                                     impl_->twC2C[{backend::bluesteinM(n), kColsE}], t.chirp, t.filt, s))
+            return -5;
+        return 0;
+    }
     int e = 0, cta = 0;
     if (resolve(backend::kC2C, n, &e, &cta)) return -1;
     if (e > 0) {

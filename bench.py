@@ -285,7 +285,8 @@ def extra_measurements(dev, stream):
     """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores vs fp32 at the
     largest power-of-16 grid points; long C2C forward + backward (batch*n = 2^26; single pass up
     to n = 16384, four-step above); 2-D C2C at the reference's planned 2-D / range-Doppler shapes
-    and transforms along a middle axis; real transforms forward + adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
+    and transforms along a middle axis; any-length C2C (Bluestein); real transforms forward +
+    adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
     events on `stream` around one replay of a CUDA graph holding 20 launches (after 3 warm-up
     launches), and the error against FP64 on sampled rows."""
     import torch
@@ -386,6 +387,19 @@ def extra_measurements(dev, stream):
         out["c2c_2d"][f"axis_n{n}_outer{outer}_inner{inner}"] = {
             "gbs": round(16 * n * outer * inner / ms / 1e6, 1),
             "frac": round(16 * n * outer * inner / ms / 1e6 / peak, 4), "rel_l2": err, "passes": 1}
+        del x, y
+    # ---- any-length C2C (Bluestein, one kernel), batch * n ~ 2^25
+    out["c2c_any_length"] = {}
+    for n in (1000, 3000, 8191):
+        b = (1 << 25) // n
+        g = torch.Generator(device=dev).manual_seed(n)
+        x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.empty_like(x)
+        plan = bfly.plan_for(dev, n)
+        ms = timed(lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh))
+        gbs = 16 * n * b / ms / 1e6
+        out["c2c_any_length"][f"n{n}_b{b}"] = {"gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
+                                               "rel_l2": rel(y, x), "padded_length": 1 << (2 * n - 2).bit_length()}
         del x, y
     # ---- real transforms: R2C forward and its adjoint (weighted C2R), batch 1024
     for n in (128, 1024, 4096, 8192):

@@ -187,7 +187,9 @@ public:
     // the CUDA default stream, stream() the context stream) and return; no host
     // synchronisation, no host<->device copies.
     //   direction -1 forward, +1 inverse; scale multiplies the output.
-    //   n in [32, 16384] single pass, [8192, 65536] four-step (workspace grown on demand).
+    //   n in [32, 16384] single pass, [8192, 65536] four-step (workspace grown on demand);
+    //   any other n in [2, 8192] (non-powers of two, and 2..16) by Bluestein's algorithm in
+    //   one kernel (the first call for a length builds its chirp and filter tables).
     int execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                 float scale, void* stream);
     // 2-D C2C over [batch][ny][nx] complex, rows of nx contiguous: nx-point row transforms
@@ -232,6 +234,7 @@ private:
     int prepareC2C(uint32_t n, int e);
     int prepareReal(uint32_t n);
     int prepareLong(uint32_t n);
+    int prepareBluestein(uint32_t n);
     int resolve(int kind, uint32_t n, int* e, int* cta) const;
     int execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                     float scale, void* stream, void* work);

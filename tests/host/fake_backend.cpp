@@ -141,6 +141,22 @@ int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
     return 0;
 }
 
+uint32_t bluesteinM(uint32_t n) {
+    if (n < 2 || n > kBluesteinMaxN) return 0;
+    uint32_t m = 64;
+    while (m < 2 * n - 1) m <<= 1;
+    return m;
+}
+int buildBluesteinTables(void*, void*, void*, uint32_t n, void*) { return bluesteinM(n) ? launch() : 1; }
+int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
+                    const void*, const void*, const void*, void*) {
+    if (!bluesteinM(n)) return 1;
+    if (int r = launch()) return r;
+    for (uint64_t b = 0; b < batch; ++b)
+        dft((const float*)in + b * 2 * n, (float*)out + b * 2 * n, n, inverse ? 1 : -1, scale);
+    return 0;
+}
+
 bool hasCols(uint32_t ny) { return ny >= 32 && ny <= 4096 && !(ny & (ny - 1)); }
 int launchCols(const void* in, void* out, uint32_t ny, uint32_t ncols, uint64_t pitch, uint64_t matStride,
                uint64_t mats, bool inverse, float scale, const void*, void*) {

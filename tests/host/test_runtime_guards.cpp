@@ -229,7 +229,8 @@ int main(int argc, char** argv) {
     CHECK(plan->execC2C(nullptr, dummy, 64, 1, -1, 1.f, nullptr) == -8);
     CHECK(plan->execC2C(dummy, dummy, 64, 0, -1, 1.f, nullptr) == -8);
     CHECK(plan->execC2C(dummy, dummy, 64, 1, 0, 1.f, nullptr) == -8);
-    CHECK(plan->execC2C(dummy, dummy, 96, 1, -1, 1.f, nullptr) == -8);
+    CHECK(plan->execC2C(dummy, dummy, 9000, 1, -1, 1.f, nullptr) == -8);   // above the Bluestein envelope
+    CHECK(plan->execC2C(dummy, dummy, 1, 1, -1, 1.f, nullptr) == -8);
     CHECK(plan->execC2C(dummy, dummy, 131072, 1, -1, 1.f, nullptr) == -8);
     CHECK(plan->execR2C(dummy, dummy, 32, 1, 1.f, 1.f, nullptr) == -8);
     CHECK(plan->execC2R(dummy, dummy, 16384, 1, 1.f, 1.f, 1.f, nullptr) == -8);
@@ -432,7 +433,7 @@ int main(int argc, char** argv) {
         CHECK(plan->execC2C2D(d, d, 16, 64, 1, -1, 1.f, nullptr) == -8);      // ny below 32
         CHECK(plan->execC2C2D(d, d, 8192, 64, 1, -1, 1.f, nullptr) == -8);    // ny above 4096
         CHECK(plan->execC2C2D(d, d, 48, 64, 1, -1, 1.f, nullptr) == -8);      // ny not a power of two
-        CHECK(plan->execC2C2D(d, d, 32, 96, 1, -1, 1.f, nullptr) == -8);      // nx not a power of two
+        CHECK(plan->execC2C2D(d, d, 32, 9000, 1, -1, 1.f, nullptr) == -8);    // nx beyond every row kernel
         CHECK(plan->execC2C2D(d, d, 4096, 64, 1u << 20, -1, 1.f, nullptr) == -8);   // batch*ny > 2^32-1
         CHECK(plan->execC2CAxis(d, d, 32, 0, 3, -1, 1.f, nullptr) == -8);
         CHECK(plan->execC2CAxis(d, d, 32, 1, 0, -1, 1.f, nullptr) == -8);
