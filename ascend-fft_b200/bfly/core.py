@@ -159,6 +159,15 @@ class Plan:
         return self._lib.bfly_plan_exec_c2c_axis_async(self._h, d_in, d_out, n, outer, inner,
                                                        direction, scale, stream or None)
 
+    def exec_stft(self, d_sig: int, d_out: int, n: int, signals: int, sig_len: int, hop: int,
+                  center: bool = True, d_window: int = 0, stream: int = 0):
+        """STFT into [signals][frames][n/2+1] complex64; returns (status, frames)."""
+        frames = C.c_uint64(0)
+        rc = self._lib.bfly_plan_exec_stft_async(self._h, d_sig, d_out, n, signals, sig_len, hop,
+                                                 1 if center else 0, d_window or None, C.byref(frames),
+                                                 stream or None)
+        return rc, frames.value
+
     def exec_r2c(self, d_in: int, d_out: int, n: int, batch: int, s_edge: float = 1.0,
                  s_int: float = 1.0, stream: int = 0) -> int:
         return self._lib.bfly_plan_exec_r2c_async(self._h, d_in, d_out, n, batch, s_edge, s_int,

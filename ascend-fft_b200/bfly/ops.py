@@ -6,6 +6,9 @@ hand-written adjoints behind torch.autograd.Function:
                             over the contiguous [outer][n][inner] view)
     fft2(x) / ifft2(x)      complex64 [..., ny, nx]: row pass (nx as fft) + column pass
                             (ny in 32..4096)
+    stft(x, n_fft, ...)     float32 [..., L] -> complex64 [..., n_fft/2+1, frames], torch.stft's
+                            arguments and defaults (centred reflect padding, hop n_fft/4); framing,
+                            window and one-sided transform in one kernel
     rfft(x)                 float32 [..., n] -> complex64 [..., n/2+1], n in 64..8192
     irfft(X, n)             complex64 [..., n/2+1] -> float32 [..., n]
 
@@ -294,6 +297,67 @@ def ifft(x: torch.Tensor, norm: str | None = None, dim: int = -1) -> torch.Tenso
     if dim % max(x.dim(), 1) != x.dim() - 1:
         return _FFTAxis.apply(x, dim, 1, _scale(norm, x.shape[dim], False))
     return _FFT.apply(x, 1, _scale(norm, x.shape[-1], False))
+
+
+class _STFT(torch.autograd.Function):
+    """Framing + window + R2C in one kernel; the window is a constant (no gradient)."""
+
+    @staticmethod
+    def forward(ctx, x, n, hop, center, window):
+        signals, length = x.shape
+        frames = (1 + length // hop) if center else (1 + (length - n) // hop)
+        y = torch.empty(signals, frames, n // 2 + 1, dtype=torch.complex64, device=x.device)
+        rc, got = plan_for(x.device, n, "real").exec_stft(
+            x.data_ptr(), y.data_ptr(), n, signals, length, hop, center,
+            window.data_ptr() if window is not None else 0, _stream(x))
+        if rc:
+            raise BflyError(f"exec_stft(n={n}, signals={signals}, length={length}, hop={hop})", rc)
+        assert got == frames
+        ctx.n, ctx.hop, ctx.center, ctx.length = n, hop, center, length
+        ctx.save_for_backward(window)
+        return y
+
+    @staticmethod
+    def backward(ctx, g):
+        (window,) = ctx.saved_tensors
+        n, hop, length = ctx.n, ctx.hop, ctx.length
+        signals, frames = g.shape[0], g.shape[1]
+        # adjoint of each frame's one-sided transform (the weighted C2R of rfft's backward)
+        fr = c2r(g.contiguous().reshape(signals * frames, n // 2 + 1), n, 1.0, 0.5, 1.0)
+        fr = fr.reshape(signals, frames, n)
+        if window is not None:
+            fr = fr * window
+        pad = n // 2 if ctx.center else 0
+        padded = length + 2 * pad
+        gp = torch.nn.functional.fold(fr.transpose(1, 2), output_size=(1, padded), kernel_size=(1, n),
+                                      stride=(1, hop)).reshape(signals, padded)
+        gx = gp[:, pad:pad + length].clone()
+        if pad:   # reflected samples: x[-i] = x[i], x[L-1+i] = x[L-1-i]
+            gx[:, 1:pad + 1] += gp[:, :pad].flip(-1)
+            gx[:, length - 1 - pad:length - 1] += gp[:, pad + length:].flip(-1)
+        return gx, None, None, None, None
+
+
+def stft(x: torch.Tensor, n_fft: int, hop_length: int | None = None, window: torch.Tensor | None = None,
+         center: bool = True, pad_mode: str = "reflect", normalized: bool = False,
+         onesided: bool = True, return_complex: bool = True) -> torch.Tensor:
+    """torch.stft on the fused kernel: float32 [..., L] -> complex64 [..., n_fft/2+1, frames]."""
+    _need_cuda(x, torch.float32, "stft")
+    if not return_complex or not onesided:
+        raise ValueError("stft: only onesided=True, return_complex=True are supported")
+    if center and pad_mode != "reflect":
+        raise ValueError("stft: only pad_mode='reflect' is supported")
+    hop = hop_length if hop_length is not None else n_fft // 4
+    if window is not None:
+        _need_cuda(window, torch.float32, "stft window")
+        if window.shape != (n_fft,):
+            raise ValueError(f"stft: window must have shape ({n_fft},)")
+        window = window.contiguous()
+    if normalized:
+        window = (window if window is not None else torch.ones(n_fft, device=x.device)) * n_fft ** -0.5
+    lead = x.shape[:-1]
+    y = _STFT.apply(x.contiguous().reshape(-1, x.shape[-1]), n_fft, hop, center, window)
+    return y.reshape(*lead, y.shape[-2], y.shape[-1]).transpose(-1, -2)
 
 
 def _need_2d(x: torch.Tensor, what: str):

@@ -84,6 +84,16 @@ int buildBluesteinTables(void* chirp, void* filt, void* scratch, uint32_t n, voi
 int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
                     const void* tw, const void* chirp, const void* filt, void* stream);
 
+// STFT: `signals` real signals of sigLen samples (signal s at s*sigStride floats), frames of n
+// samples every `hop` (centred with reflect padding when `center`), times `window` (n floats,
+// or null for none), R2C of each frame into out[s][f][n/2+1].  n a power of two in
+// [kStftMinN, kStftMaxN]; tw = Stockham table (n/2, 16), twr = W_n^k, k <= n/2.
+constexpr uint32_t kStftMinN = 64, kStftMaxN = 8192;
+bool hasStft(uint32_t n);
+int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal,
+               uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,
+               const void* tw, const void* twr, void* stream);
+
 // Column FFTs: ny-point transforms down the ncols columns of `mats` row-major matrices,
 // element (m, i, col) at m*matStride + i*pitch + col (float2 units).  ny in 32..4096;
 // tw = Stockham table (ny, 16); in == out allowed.

@@ -180,6 +180,13 @@ int bfly_plan_exec_c2c_axis_async(bfly_plan* plan, const void* d_in, void* d_out
     return p.execC2CAxis(d_in, d_out, n, outer, inner, direction, scale, stream);
 }
 
+int bfly_plan_exec_stft_async(bfly_plan* plan, const void* d_sig, void* d_out, uint32_t n,
+                              uint64_t signals, uint64_t sig_len, uint32_t hop, int center,
+                              const void* d_window, uint64_t* frames, void* stream) {
+    PLAN_OR_FAIL();
+    return p.execStft(d_sig, d_out, n, signals, sig_len, hop, center != 0, d_window, frames, stream);
+}
+
 int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, float s_edge, float s_int, void* stream) {
     PLAN_OR_FAIL();

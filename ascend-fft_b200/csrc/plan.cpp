@@ -662,6 +662,20 @@ int Plan::execC2CAxis(const void* dIn, void* dOut, uint32_t n, uint64_t outer, u
     return execCols(dIn, dOut, n, outer, (uint32_t)inner, inner, direction > 0, scale, stream);
 }
 
+int Plan::execStft(const void* dSig, void* dOut, uint32_t n, uint64_t signals, uint64_t sigLen,
+                   uint32_t hop, bool center, const void* dWindow, uint64_t* framesOut, void* stream) {
+    if (!impl_ || !dSig || !dOut || signals == 0 || hop == 0 || !backend::hasStft(n)) return -8;
+    if (center ? sigLen <= n / 2 : sigLen < n) return -8;
+    const uint64_t frames = center ? 1 + sigLen / hop : 1 + (sigLen - n) / hop;
+    if (frames > 0xFFFFFFFFull || signals > (~0ull) / frames) return -8;
+    if (framesOut) *framesOut = frames;
+    if (prepareC2C(n / 2, kColsE) || prepareReal(n)) return -2;
+    if (backend::launchStft(dSig, dOut, n, signals, (uint32_t)frames, sigLen, sigLen, hop, center, dWindow,
+                            impl_->twC2C[{n / 2, kColsE}], impl_->twReal[n], stream))
+        return -5;
+    return 0;
+}
+
 int Plan::execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
                   float sInt, void* stream) {
     if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull) return -8;

@@ -285,8 +285,8 @@ def extra_measurements(dev, stream):
     """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores vs fp32 at the
     largest power-of-16 grid points; long C2C forward + backward (batch*n = 2^26; single pass up
     to n = 16384, four-step above); 2-D C2C at the reference's planned 2-D / range-Doppler shapes
-    and transforms along a middle axis; any-length C2C (Bluestein); real transforms forward +
-    adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
+    and transforms along a middle axis; any-length C2C (Bluestein); STFT; real transforms
+    forward + adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
     events on `stream` around one replay of a CUDA graph holding 20 launches (after 3 warm-up
     launches), and the error against FP64 on sampled rows."""
     import torch
@@ -400,6 +400,27 @@ def extra_measurements(dev, stream):
         gbs = 16 * n * b / ms / 1e6
         out["c2c_any_length"][f"n{n}_b{b}"] = {"gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
                                                "rel_l2": rel(y, x), "padded_length": 1 << (2 * n - 2).bit_length()}
+        del x, y
+    # ---- STFT (frame gather + Hann window + one-sided transform in one kernel), 4 signals of
+    # 2^24 samples, centred; bytes counted per frame as the reference's dense-frame R2C proxy
+    out["stft"] = {}
+    plan = bfly.plan_for(dev, 1024, "real")
+    for n, hop in ((256, 64), (1024, 256), (4096, 1024)):
+        L, S = 1 << 24, 4
+        g = torch.Generator(device=dev).manual_seed(n)
+        x = torch.randn(S, L, device=dev, generator=g)
+        w = torch.hann_window(n, device=dev)
+        frames = 1 + L // hop
+        y = torch.empty(S, frames, n // 2 + 1, dtype=torch.complex64, device=dev)
+        ms = timed(lambda: plan.exec_stft(x.data_ptr(), y.data_ptr(), n, S, L, hop, True, w.data_ptr(), sh))
+        fb = S * frames * (4 * n + 8 * (n // 2 + 1))
+        # the first 8 frames depend only on a prefix (left reflect padding + 8 hops + one frame)
+        ref = torch.stft(x[:1, :16 * n].double(), n, hop_length=hop, window=w.double(), return_complex=True)[..., :8]
+        got = y[:1, :8].transpose(-1, -2).to(torch.complex128)
+        err = float((torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)).item())
+        out["stft"][f"n{n}_hop{hop}_S{S}_L{L}"] = {"frame_gbs": round(fb / ms / 1e6, 1),
+                                                    "frac": round(fb / ms / 1e6 / peak, 4), "rel_l2": err,
+                                                    "frames": S * frames}
         del x, y
     # ---- real transforms: R2C forward and its adjoint (weighted C2R), batch 1024
     for n in (128, 1024, 4096, 8192):

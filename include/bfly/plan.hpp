@@ -202,6 +202,13 @@ public:
     // inner > 1 runs the column kernel (n in [32, 4096]).  dIn == dOut allowed.
     int execC2CAxis(const void* dIn, void* dOut, uint32_t n, uint64_t outer, uint64_t inner,
                     int direction, float scale, void* stream);
+    // STFT of `signals` contiguous real signals of sigLen fp32 samples: frames of n samples
+    // (n a power of two in [64, 8192]) every `hop`, centred with reflect padding when
+    // `center` (then sigLen > n/2), times dWindow (n floats, or null), R2C of every frame into
+    // dOut = [signals][frames][n/2+1] complex, frames = center ? 1 + sigLen/hop
+    // : 1 + (sigLen-n)/hop.  *framesOut receives the frame count (may be null).
+    int execStft(const void* dSig, void* dOut, uint32_t n, uint64_t signals, uint64_t sigLen, uint32_t hop,
+                 bool center, const void* dWindow, uint64_t* framesOut, void* stream);
     // R2C [batch][n] -> [batch][n/2+1] complex, bins scaled by (sEdge at 0 and n/2, sInt
     // elsewhere); sEdge = sInt = 1 is the plain transform.
     int execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,

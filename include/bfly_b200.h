@@ -132,6 +132,16 @@ int bfly_plan_exec_c2c_2d_async(bfly_plan* plan, const void* d_in, void* d_out, 
 int bfly_plan_exec_c2c_axis_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                                   uint64_t outer, uint64_t inner, int direction, float scale,
                                   void* stream);
+/* New: STFT of `signals` contiguous fp32 signals of sig_len samples: frames of n samples (n a
+ * power of two in [64, 8192]) every `hop`, centred with reflect padding when center != 0
+ * (sig_len > n/2; torch.stft's defaults), times d_window (n floats, or NULL), one-sided
+ * spectrum of every frame into d_out = [signals][frames][n/2+1] complex;
+ * frames = center ? 1 + sig_len/hop : 1 + (sig_len-n)/hop, returned in *frames (may be NULL).
+ * The reference measures STFT only as a dense-frame R2C proxy (docs/testing.md:118,
+ * config/test_matrix.json); framing, window and overlap run here inside one kernel. */
+int bfly_plan_exec_stft_async(bfly_plan* plan, const void* d_sig, void* d_out, uint32_t n,
+                              uint64_t signals, uint64_t sig_len, uint32_t hop, int center,
+                              const void* d_window, uint64_t* frames, void* stream);
 /* R2C [batch][n] -> [batch][n/2+1] complex, n in [64, 8192]; bins 0 and n/2 scaled by
  * s_edge, the others by s_int (1, 1 for the plain transform). */
 int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,

@@ -157,6 +157,32 @@ int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool 
     return 0;
 }
 
+bool hasStft(uint32_t n) { return n >= kStftMinN && n <= kStftMaxN && !(n & (n - 1)); }
+int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal,
+               uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,
+               const void*, const void*, void*) {
+    if (!hasStft(n)) return 1;
+    if (int r = launch()) return r;
+    const float* x = (const float*)sig;
+    const float* w = (const float*)window;
+    std::vector<float> frame(2 * n), spec(2 * n);
+    for (uint64_t s = 0; s < signals; ++s)
+        for (uint32_t f = 0; f < framesPerSignal; ++f) {
+            const long long start = (long long)f * hop - (center ? n / 2 : 0);
+            for (uint32_t j = 0; j < n; ++j) {
+                long long i = start + j;
+                if (i < 0) i = -i;
+                if (i >= (long long)sigLen) i = 2 * ((long long)sigLen - 1) - i;
+                frame[2 * j] = x[s * sigStride + i] * (w ? w[j] : 1.f);
+                frame[2 * j + 1] = 0.f;
+            }
+            dft(frame.data(), spec.data(), n, -1, 1.f);
+            float* o = (float*)out + 2 * ((s * framesPerSignal + f) * (n / 2 + 1));
+            std::memcpy(o, spec.data(), (n / 2 + 1) * 8);
+        }
+    return 0;
+}
+
 bool hasCols(uint32_t ny) { return ny >= 32 && ny <= 4096 && !(ny & (ny - 1)); }
 int launchCols(const void* in, void* out, uint32_t ny, uint32_t ncols, uint64_t pitch, uint64_t matStride,
                uint64_t mats, bool inverse, float scale, const void*, void*) {

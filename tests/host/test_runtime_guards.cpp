@@ -442,6 +442,51 @@ int main(int argc, char** argv) {
         CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
     }
 
+    {   // STFT: frame count, centred reflect padding and window against a direct DFT
+        const uint32_t n = 64, hop = 24;
+        const uint64_t len = 200, signals = 2;
+        std::vector<float> sig(len * signals), win(n);
+        for (size_t i = 0; i < sig.size(); ++i) sig[i] = (float)std::cos(0.05 * i * i / 7.0 + i % 3);
+        for (uint32_t j = 0; j < n; ++j) win[j] = (float)(0.5 - 0.5 * std::cos(2 * M_PI * j / n));
+        for (bool center : {true, false}) {
+            const uint64_t frames = center ? 1 + len / hop : 1 + (len - n) / hop;
+            std::vector<float> spec(2 * (n / 2 + 1) * frames * signals);
+            uint64_t got = 0;
+            CHECK(plan->execStft(sig.data(), spec.data(), n, signals, len, hop, center, win.data(), &got, nullptr) == 0);
+            CHECK(got == frames);
+            double e = 0;
+            for (uint64_t s2 = 0; s2 < signals; ++s2)
+                for (uint64_t f = 0; f < frames; ++f)
+                    for (uint32_t k = 0; k <= n / 2; ++k) {
+                        double re = 0, im = 0;
+                        for (uint32_t j = 0; j < n; ++j) {
+                            long long i = (long long)(f * hop + j) - (center ? n / 2 : 0);
+                            if (i < 0) i = -i;
+                            if (i >= (long long)len) i = 2 * ((long long)len - 1) - i;
+                            const double v = sig[s2 * len + i] * win[j];
+                            const double a = -2 * M_PI * (double)((j * k) % n) / n;
+                            re += v * std::cos(a);
+                            im += v * std::sin(a);
+                        }
+                        const size_t o = 2 * ((s2 * frames + f) * (n / 2 + 1) + k);
+                        e = std::max(e, std::max(std::fabs(spec[o] - re), std::fabs(spec[o + 1] - im)));
+                    }
+            CHECK(e < 1e-3);
+        }
+        const int allocBefore = fake::allocations, launchBefore = fake::launches;
+        float* d = sig.data();
+        uint64_t fr = 0;
+        CHECK(plan->execStft(nullptr, d, 64, 1, 200, 16, true, nullptr, &fr, nullptr) == -8);
+        CHECK(plan->execStft(d, d, 96, 1, 200, 16, true, nullptr, &fr, nullptr) == -8);     // not a power of two
+        CHECK(plan->execStft(d, d, 32, 1, 200, 16, true, nullptr, &fr, nullptr) == -8);     // below 64
+        CHECK(plan->execStft(d, d, 16384, 1, 20000, 16, true, nullptr, &fr, nullptr) == -8);
+        CHECK(plan->execStft(d, d, 64, 1, 200, 0, true, nullptr, &fr, nullptr) == -8);      // hop 0
+        CHECK(plan->execStft(d, d, 64, 0, 200, 16, true, nullptr, &fr, nullptr) == -8);     // no signals
+        CHECK(plan->execStft(d, d, 64, 1, 32, 16, true, nullptr, &fr, nullptr) == -8);      // reflect needs len > n/2
+        CHECK(plan->execStft(d, d, 64, 1, 63, 16, false, nullptr, &fr, nullptr) == -8);     // shorter than a frame
+        CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
+    }
+
     plan.reset();
     best.reset();
     cached.reset();
