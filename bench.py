@@ -639,15 +639,44 @@ def run_ours(args):
 
 def run_case(spec: str, reps: int):
     """Launch one kernel configuration `reps` times without timing (for ncu captures):
-    spec = kind:n:batch with kind in c2c, c2c_inv, tc2, tc3 (tensor-core splits), r2c, c2r,
-    or ragged:grid:CAP."""
+    spec = kind:n:batch with kind in c2c, c2c_inv (any n: non-powers of two run the Bluestein
+    kernel), tc2, tc3 (tensor-core splits), r2c, c2r, cluster (long C2C on the cluster
+    schedule), or ragged:grid:CAP; or cols:NY:NCOLS:MATS (column kernel), c2d:NY:NX:B (2-D),
+    stft:N:HOP:LEN (4 signals, centred, Hann window)."""
     import torch
     import bfly
-    kind, n, b = spec.split(":")
+    parts = spec.split(":")
+    kind = parts[0]
     dev = torch.device("cuda", 0)
     ctx = bfly.Context()
     assert ctx.init() == 0
     plan = ctx.make_plan()
+    if kind in ("cols", "c2d", "stft"):
+        a, b2, c = (int(v) for v in parts[1:4])
+        g = torch.Generator(device=dev).manual_seed(a + b2 + c)
+        if kind == "cols":     # NY-point transforms down NCOLS columns of MATS matrices
+            x = torch.randn(c, a, b2, dtype=torch.complex64, device=dev, generator=g)
+            y = torch.empty_like(x)
+            call = lambda: plan.exec_c2c_axis(x.data_ptr(), y.data_ptr(), a, c, b2, -1, 1.0, 0)
+        elif kind == "c2d":
+            x = torch.randn(c, a, b2, dtype=torch.complex64, device=dev, generator=g)
+            y = torch.empty_like(x)
+            call = lambda: plan.exec_c2c_2d(x.data_ptr(), y.data_ptr(), a, b2, c, -1, 1.0, 0)
+        else:                  # stft:N:HOP:LEN
+            x = torch.randn(4, c, device=dev, generator=g)
+            w = torch.hann_window(a, device=dev)
+            y = torch.empty(4, 1 + c // b2, a // 2 + 1, dtype=torch.complex64, device=dev)
+            call = lambda: plan.exec_stft(x.data_ptr(), y.data_ptr(), a, 4, c, b2, True, w.data_ptr())[0]
+        for _ in range(reps):
+            r = call()
+            if r:
+                raise SystemExit(f"{spec}: status {r}")
+        torch.cuda.synchronize()
+        print(f"case {spec} x{reps} ok")
+        return 0
+    n, b = parts[1], parts[2]
+    if kind == "cluster":
+        plan = ctx.make_plan("r16_cta256_shared_fp32_cluster", 8192, 1)
     if kind == "ragged":   # ragged:grid:CAP -> the 49-point grid with batch capped at CAP
         cap = int(b)
         bufs = []
@@ -666,7 +695,7 @@ def run_case(spec: str, reps: int):
         return 0
     n, b = int(n), int(b)
     g = torch.Generator(device=dev).manual_seed(grid_seed(n, b))
-    if kind in ("c2c", "c2c_inv"):
+    if kind in ("c2c", "c2c_inv", "cluster"):
         x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
         y = torch.empty_like(x)
         call = lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, 1 if kind == "c2c_inv" else -1, 1.0, 0)
@@ -695,7 +724,7 @@ def run_case(spec: str, reps: int):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default=None, help="kind:n:batch, launch only that kernel (for ncu)")
+    ap.add_argument("--case", default=None, help="kind:n:batch (see run_case), launch only that kernel (for ncu)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--no-extras", action="store_true", help="skip the split-BF16 / fwd+bwd sub-measurements")
     ap.add_argument("--gpus", type=int, default=1)
