@@ -24,6 +24,11 @@ int releaseHost(void* ptr);
 int copyH2D(void* dst, const void* src, size_t bytes, void* stream);
 int copyD2H(void* dst, const void* src, size_t bytes, void* stream);
 int streamSync(void* stream);
+// Ordering between streams (events without timing).
+int eventCreate(void** event);
+int eventDestroy(void* event);
+int eventRecord(void* event, void* stream);
+int streamWaitEvent(void* stream, void* event);   // later work on `stream` waits for `event`
 
 // Device-side elapsed time between start() and stop() on one stream (CUDA events).
 struct Timer;

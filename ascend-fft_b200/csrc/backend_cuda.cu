@@ -50,6 +50,17 @@ int copyD2H(void* dst, const void* src, size_t bytes, void* stream) {
     return rc(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S(stream)));
 }
 int streamSync(void* stream) { return rc(cudaStreamSynchronize(S(stream))); }
+int eventCreate(void** event) {
+    cudaEvent_t e = nullptr;
+    const int r = rc(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    *event = e;
+    return r;
+}
+int eventDestroy(void* event) { return rc(cudaEventDestroy(static_cast<cudaEvent_t>(event))); }
+int eventRecord(void* event, void* stream) { return rc(cudaEventRecord(static_cast<cudaEvent_t>(event), S(stream))); }
+int streamWaitEvent(void* stream, void* event) {
+    return rc(cudaStreamWaitEvent(S(stream), static_cast<cudaEvent_t>(event), 0));
+}
 
 struct Timer {
     cudaEvent_t a = nullptr, b = nullptr;

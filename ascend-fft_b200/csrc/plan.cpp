@@ -348,7 +348,8 @@ struct Plan::Impl {
     void* devWork = nullptr;
     size_t devInCap = 0, devOutCap = 0, devWorkCap = 0;
     backend::Timer* timer = nullptr;
-    void* aux[2] = {nullptr, nullptr};   // extra streams of the pipelined host round trip
+    void* aux[2] = {nullptr, nullptr};   // upload / download streams of the pipelined host round trip
+    void* ev[2] = {nullptr, nullptr};    // chunk uploaded / chunk transformed
     void* tcTable[4] = {nullptr, nullptr, nullptr, nullptr};   // split DFT-16 operand per term count
     struct Chirp {
         void* chirp = nullptr;   // c[j] = exp(-i*pi*j^2/n), j < n
@@ -373,6 +374,8 @@ Plan::~Plan() {
     backend::timerDestroy(impl_->timer);
     for (void* st : impl_->aux)
         if (st) backend::streamDestroy(st);
+    for (void* e : impl_->ev)
+        if (e) backend::eventDestroy(e);
     for (void* t : impl_->tcTable)
         if (t) backend::release(t);
     for (auto& kv : impl_->bluestein) {
@@ -704,10 +707,10 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
 }
 
 // Body of the synchronous host-pointer entry points: upload, enqueue, synchronise, download.
-// Transfers above kPipelineBytes are cut into row chunks of about kChunkBytes that rotate over
-// three streams, so the H2D of one chunk, the kernels of another and the D2H of a third
-// overlap (two copy engines).  enqueue() returns an exec status: -2 prepare and -3 alloc pass
-// through, any other failure is a launch failure (-5).
+// Transfers above kPipelineBytes are cut into row chunks of about kChunkBytes that flow through
+// an upload stream, the context stream and a download stream, so the H2D of one chunk, the
+// kernels of another and the D2H of a third overlap (two copy engines).  enqueue() returns an
+// exec status: -2 prepare and -3 alloc pass through, any other failure is a launch failure (-5).
 constexpr size_t kPipelineBytes = 4u << 20, kChunkBytes = 4u << 20;
 
 template <class Enqueue>
@@ -717,40 +720,48 @@ int Plan::roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRo
     const size_t inBytes = inRowBytes * batch, outBytes = outRowBytes * batch;
     if (ensureBuf(&im->devIn, &im->devInCap, inBytes)) return -3;
     if (ensureBuf(&im->devOut, &im->devOutCap, outBytes)) return -3;
-    void* streams[3] = {stream_, nullptr, nullptr};
-    int nstreams = 1;
-    uint32_t chunk = batch;
+    bool pipelined = false;
     if (inBytes + outBytes > kPipelineBytes) {
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < 2; ++i) {
             if (!im->aux[i] && backend::streamCreate(&im->aux[i])) im->aux[i] = nullptr;
-        if (im->aux[0] && im->aux[1]) {
-            streams[1] = im->aux[0];
-            streams[2] = im->aux[1];
-            nstreams = 3;
-            const size_t row = inRowBytes > outRowBytes ? inRowBytes : outRowBytes;
-            chunk = (uint32_t)std::max<size_t>(1, kChunkBytes / row);
+            if (!im->ev[i] && backend::eventCreate(&im->ev[i])) im->ev[i] = nullptr;
         }
+        pipelined = im->aux[0] && im->aux[1] && im->ev[0] && im->ev[1];
     }
-    int k = 0;
-    for (uint32_t r0 = 0; r0 < batch; r0 += chunk, ++k) {
+    if (!pipelined) {   // one stream: upload, transform, download
+        if (backend::copyH2D(im->devIn, in, inBytes, stream_)) return -4;
+        const int lrc = enqueue(im->devIn, im->devOut, 0u, batch, stream_);
+        if (lrc == -2 || lrc == -3) return lrc;
+        if (lrc) return -5;
+        if (backend::streamSync(stream_)) return -6;
+        if (backend::copyD2H(out, im->devOut, outBytes, stream_)) return -7;
+        return backend::streamSync(stream_) ? -7 : 0;
+    }
+    // Chunks of rows through three streams, one per stage: uploads on aux[0], transforms on the
+    // context stream, downloads on aux[1], each chunk's stages ordered by two events.  Both copy
+    // directions then stream back to back and overlap each other and the kernels.
+    void* sIn = im->aux[0];
+    void* sOut = im->aux[1];
+    const size_t row = inRowBytes > outRowBytes ? inRowBytes : outRowBytes;
+    const uint32_t chunk = (uint32_t)std::max<size_t>(1, kChunkBytes / row);
+    for (uint32_t r0 = 0; r0 < batch; r0 += chunk) {
         const uint32_t rows = std::min(chunk, batch - r0);
-        void* st = streams[k % nstreams];
         char* di = static_cast<char*>(im->devIn) + (size_t)r0 * inRowBytes;
         char* dout = static_cast<char*>(im->devOut) + (size_t)r0 * outRowBytes;
         if (backend::copyH2D(di, reinterpret_cast<const char*>(in) + (size_t)r0 * inRowBytes,
-                             (size_t)rows * inRowBytes, st))
+                             (size_t)rows * inRowBytes, sIn))
             return -4;
-        const int lrc = enqueue(di, dout, r0, rows, st);
+        if (backend::eventRecord(im->ev[0], sIn) || backend::streamWaitEvent(stream_, im->ev[0])) return -6;
+        const int lrc = enqueue(di, dout, r0, rows, stream_);
         if (lrc == -2 || lrc == -3) return lrc;
         if (lrc) return -5;
-        if (nstreams == 1 && backend::streamSync(st)) return -6;
+        if (backend::eventRecord(im->ev[1], stream_) || backend::streamWaitEvent(sOut, im->ev[1])) return -6;
         if (backend::copyD2H(reinterpret_cast<char*>(out) + (size_t)r0 * outRowBytes, dout,
-                             (size_t)rows * outRowBytes, st))
+                             (size_t)rows * outRowBytes, sOut))
             return -7;
     }
-    for (int i = 0; i < nstreams; ++i)
-        if (backend::streamSync(streams[i])) return nstreams == 1 ? -7 : -6;
-    return 0;
+    if (backend::streamSync(sIn) || backend::streamSync(stream_)) return -6;
+    return backend::streamSync(sOut) ? -6 : 0;
 }
 
 int Plan::run(const float* in, float* out, uint32_t n, uint32_t batch) {

@@ -61,6 +61,10 @@ int deviceName(int, char* buf, size_t cap) { std::strncpy(buf, "fake", cap); ret
 int smCount(int, int* count) { *count = 148; return 0; }
 int streamCreate(void** s) { ++fake::streamsCreated; *s = reinterpret_cast<void*>(0x1); return 0; }
 int streamDestroy(void*) { ++fake::streamsDestroyed; return 0; }
+int eventCreate(void** e) { *e = reinterpret_cast<void*>(0x2); return 0; }
+int eventDestroy(void*) { return 0; }
+int eventRecord(void*, void*) { return 0; }
+int streamWaitEvent(void*, void*) { return 0; }
 int alloc(void** p, size_t bytes) {
     ++fake::allocations;
     if (fake::allocations == fake::failAllocation) { *p = nullptr; return 2; }
