@@ -32,6 +32,7 @@ SIGNATURES = {
     "bfly_plan_candidate_id": (C.c_int, [c_plan, C.c_char_p, C.c_size_t]),
     "bfly_plan_prepare": (C.c_int, [c_plan, C.c_uint32, C.c_uint32]),
     "bfly_plan_run_c2c": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]),
+    "bfly_plan_run_c2c_many": (C.c_int, [c_plan, C.c_void_p, C.c_size_t]),
     "bfly_plan_run_r2c": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]),
     "bfly_plan_run_c2r": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]),
     "bfly_plan_measure": (C.c_int, [c_plan, C.c_uint32, C.c_uint32, C.c_void_p]),
@@ -75,6 +76,12 @@ class RaggedRequest(C.Structure):
     _fields_ = [("d_in", C.c_void_p), ("d_out", C.c_void_p), ("n", C.c_uint32),
                 ("direction", C.c_int32), ("batch", C.c_uint64), ("scale", C.c_float),
                 ("reserved", C.c_uint32)]
+
+
+class HostRequest(C.Structure):
+    """bfly_host_request of include/bfly_b200.h."""
+    _fields_ = [("in_", C.c_void_p), ("out", C.c_void_p), ("n", C.c_uint32), ("batch", C.c_uint32),
+                ("direction", C.c_int32), ("scale", C.c_float)]
 
 
 class Metric(C.Structure):

@@ -123,6 +123,18 @@ class Plan:
     def run(self, x: np.ndarray, out: np.ndarray, n: int, batch: int) -> int:
         return self._lib.bfly_plan_run_c2c(self._h, _ptr(x), _ptr(out), n, batch)
 
+    def run_many(self, requests) -> int:
+        """Host-to-host C2C of many requests in one pipelined call.  `requests`: iterable of
+        (x, out, n, batch) or (x, out, n, batch, direction, scale) with C-contiguous numpy
+        float32 [batch][2n] arrays (pinned memory for full PCIe bandwidth)."""
+        reqs = list(requests)
+        arr = (_lib.HostRequest * len(reqs))()
+        for i, r in enumerate(reqs):
+            x, out, n, batch = r[:4]
+            direction, scale = (r[4], r[5]) if len(r) > 4 else (-1, 1.0)
+            arr[i] = _lib.HostRequest(_ptr(x), _ptr(out), n, batch, direction, scale)
+        return self._lib.bfly_plan_run_c2c_many(self._h, arr if reqs else None, len(reqs))
+
     def run_r2c(self, x: np.ndarray, out: np.ndarray, n: int, batch: int) -> int:
         return self._lib.bfly_plan_run_r2c(self._h, _ptr(x), _ptr(out), n, batch)
 

@@ -127,6 +127,15 @@ int bfly_plan_run_c2c(bfly_plan* plan, const float* in, float* out, uint32_t n, 
     return p.run(in, out, n, batch);
 }
 
+int bfly_plan_run_c2c_many(bfly_plan* plan, const bfly_host_request* reqs, size_t count) {
+    PLAN_OR_FAIL();
+    if (!reqs || count == 0) return -8;
+    std::vector<bfly::HostRequest> rs(count);
+    for (size_t i = 0; i < count; ++i)
+        rs[i] = {reqs[i].in, reqs[i].out, reqs[i].n, reqs[i].batch, reqs[i].direction, reqs[i].scale};
+    return p.runMany(rs.data(), count);
+}
+
 int bfly_plan_run_r2c(bfly_plan* plan, const float* in, float* out, uint32_t n, uint32_t batch) {
     PLAN_OR_FAIL();
     return p.runR2C(in, out, n, batch);

@@ -707,11 +707,17 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
 }
 
 // Body of the synchronous host-pointer entry points: upload, enqueue, synchronise, download.
-// Transfers above kPipelineBytes are cut into row chunks of about kChunkBytes that flow through
-// an upload stream, the context stream and a download stream, so the H2D of one chunk, the
-// kernels of another and the D2H of a third overlap (two copy engines).  enqueue() returns an
-// exec status: -2 prepare and -3 alloc pass through, any other failure is a launch failure (-5).
-constexpr size_t kPipelineBytes = 4u << 20, kChunkBytes = 4u << 20;
+// Transfers above kPipelineBytes are cut into row chunks that flow through an upload stream, the
+// context stream and a download stream, so the H2D of one chunk, the kernels of another and the
+// D2H of a third overlap (two copy engines).  Chunk size trades pipeline fill against the gap
+// each chunk boundary leaves on the copy engines: on B200 over PCIe 5 (99 GB/s both directions
+// together) 4 MB chunks reached 81 GB/s and 16 MB chunks 92 GB/s, so a transfer is cut into
+// quarters of 2..16 MB and the many-request call uses 16 MB.  enqueue() returns an exec status:
+// -2 prepare and -3 alloc pass through, any other failure is a launch failure (-5).
+constexpr size_t kPipelineBytes = 4u << 20, kChunkBytes = 16u << 20;
+static size_t chunkBytesFor(size_t bytes) {
+    return std::min<size_t>(kChunkBytes, std::max<size_t>(2u << 20, bytes / 4));
+}
 
 template <class Enqueue>
 int Plan::roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRowBytes,
@@ -743,7 +749,7 @@ int Plan::roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRo
     void* sIn = im->aux[0];
     void* sOut = im->aux[1];
     const size_t row = inRowBytes > outRowBytes ? inRowBytes : outRowBytes;
-    const uint32_t chunk = (uint32_t)std::max<size_t>(1, kChunkBytes / row);
+    const uint32_t chunk = (uint32_t)std::max<size_t>(1, chunkBytesFor(row * batch) / row);
     for (uint32_t r0 = 0; r0 < batch; r0 += chunk) {
         const uint32_t rows = std::min(chunk, batch - r0);
         char* di = static_cast<char*>(im->devIn) + (size_t)r0 * inRowBytes;
@@ -760,6 +766,98 @@ int Plan::roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRo
                              (size_t)rows * outRowBytes, sOut))
             return -7;
     }
+    if (backend::streamSync(sIn) || backend::streamSync(stream_)) return -6;
+    return backend::streamSync(sOut) ? -6 : 0;
+}
+
+int Plan::runMany(const HostRequest* reqs, size_t count) {
+    if (!impl_ || !reqs || count == 0) return -8;
+    constexpr size_t kAlign = 256;
+    auto up = [](size_t v) { return (v + kAlign - 1) / kAlign * kAlign; };
+    size_t total = 0, workElems = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const HostRequest& r = reqs[i];
+        if (!r.in || !r.out || (r.direction != -1 && r.direction != 1) || !validShape(r.n, r.batch, kExecC2C))
+            return -8;
+        total += up((size_t)r.n * r.batch * 8);
+    }
+    Impl* im = impl_.get();
+    for (size_t i = 0; i < count; ++i) {   // tables, and the four-step workspace for the largest chunk
+        const HostRequest& r = reqs[i];
+        if (pow2(r.n) && r.n >= kMinN) {
+            int e = 0, cta = 0;
+            if (resolve(backend::kC2C, r.n, &e, &cta)) return -1;
+            if (prepare(r.n, 1)) return -2;
+            if (e == 0) {
+                const size_t rows = std::min<size_t>(r.batch, std::max<size_t>(1, kChunkBytes / ((size_t)r.n * 8)));
+                workElems = std::max(workElems, rows * r.n);
+            }
+        } else if (prepareBluestein(r.n)) {
+            return -2;
+        }
+    }
+    if (ensureBuf(&im->devIn, &im->devInCap, total) || ensureBuf(&im->devOut, &im->devOutCap, total)) return -3;
+    if (workElems && ensureBuf(&im->devWork, &im->devWorkCap, workElems * 8)) return -3;
+    for (int i = 0; i < 2; ++i) {
+        if (!im->aux[i] && backend::streamCreate(&im->aux[i])) im->aux[i] = nullptr;
+        if (!im->ev[i] && backend::eventCreate(&im->ev[i])) im->ev[i] = nullptr;
+    }
+    if (!im->aux[0] || !im->aux[1] || !im->ev[0] || !im->ev[1]) return -3;
+    // Row chunks of at most kChunkBytes; consecutive pieces smaller than that are grouped up to
+    // kGroupBytes, each group sharing one upload event and one transform event (a group's
+    // copies and kernels run as three phases, so small groups keep several in flight).
+    constexpr size_t kGroupBytes = 2u << 20;
+    void* sIn = im->aux[0];
+    void* sOut = im->aux[1];
+    struct Piece {
+        const HostRequest* r;
+        size_t off;   // byte offset of the piece in devIn / devOut
+        uint32_t r0, rows;
+    };
+    std::vector<Piece> group;
+    size_t groupBytes = 0;
+    auto flush = [&]() -> int {
+        if (group.empty()) return 0;
+        for (const Piece& p : group) {
+            const size_t rowBytes = (size_t)p.r->n * 8;
+            if (backend::copyH2D(static_cast<char*>(im->devIn) + p.off,
+                                 reinterpret_cast<const char*>(p.r->in) + (size_t)p.r0 * rowBytes,
+                                 (size_t)p.rows * rowBytes, sIn))
+                return -4;
+        }
+        if (backend::eventRecord(im->ev[0], sIn) || backend::streamWaitEvent(stream_, im->ev[0])) return -6;
+        for (const Piece& p : group) {
+            const int lrc = execC2CWith(static_cast<char*>(im->devIn) + p.off, static_cast<char*>(im->devOut) + p.off,
+                                        p.r->n, p.rows, p.r->direction, p.r->scale, stream_, im->devWork);
+            if (lrc == -2 || lrc == -3) return lrc;
+            if (lrc) return -5;
+        }
+        if (backend::eventRecord(im->ev[1], stream_) || backend::streamWaitEvent(sOut, im->ev[1])) return -6;
+        for (const Piece& p : group) {
+            const size_t rowBytes = (size_t)p.r->n * 8;
+            if (backend::copyD2H(reinterpret_cast<char*>(p.r->out) + (size_t)p.r0 * rowBytes,
+                                 static_cast<char*>(im->devOut) + p.off, (size_t)p.rows * rowBytes, sOut))
+                return -7;
+        }
+        group.clear();
+        groupBytes = 0;
+        return 0;
+    };
+    size_t off = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const HostRequest& r = reqs[i];
+        const size_t rowBytes = (size_t)r.n * 8;
+        const uint32_t chunk = (uint32_t)std::max<size_t>(1, kChunkBytes / rowBytes);
+        for (uint32_t r0 = 0; r0 < r.batch; r0 += chunk) {
+            const uint32_t rows = std::min(chunk, r.batch - r0);
+            group.push_back({&r, off + (size_t)r0 * rowBytes, r0, rows});
+            groupBytes += (size_t)rows * rowBytes;
+            if (groupBytes >= kGroupBytes)
+                if (int rc = flush()) return rc;
+        }
+        off += up((size_t)r.n * r.batch * 8);
+    }
+    if (int rc = flush()) return rc;
     if (backend::streamSync(sIn) || backend::streamSync(stream_)) return -6;
     return backend::streamSync(sOut) ? -6 : 0;
 }

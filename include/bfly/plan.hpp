@@ -122,6 +122,17 @@ public:
 class Context;
 class Plan;
 
+// One request of a batched host round trip (Plan::runMany): C2C of `batch` rows of length n
+// (any execC2C length) from host `in` to host `out`, [batch][2n] interleaved fp32 each.
+struct HostRequest {
+    const float* in;
+    float* out;
+    uint32_t n;
+    uint32_t batch;
+    int direction;   // -1 forward, +1 inverse
+    float scale;
+};
+
 // One request of a ragged launch: C2C of `batch` rows of length n (32..4096, power of two)
 // between device buffers, direction -1 forward / +1 inverse, output times scale.
 struct RaggedRequest {
@@ -175,6 +186,11 @@ public:
     //   runC2R  in [batch][n+2] -> out [batch][n] real incl. 1/n, n in [64, 4096]
     // batch > 0, non-null pointers, batch*2n <= 2^32-1; otherwise -8 before any allocation.
     int run(const float* in, float* out, uint32_t n, uint32_t batch);
+    // Many host-to-host C2C requests in one synchronous call: every request is validated first
+    // (-8 before any allocation or copy), then their row chunks flow through an upload stream,
+    // the context stream and a download stream, so the copies of different requests overlap
+    // each other and the kernels.  Host buffers should be pinned for full PCIe bandwidth.
+    int runMany(const HostRequest* reqs, size_t count);
     int runR2C(const float* in, float* out, uint32_t n, uint32_t batch);
     int runC2R(const float* in, float* out, uint32_t n, uint32_t batch);
     int measure(uint32_t n, uint32_t batch, Metric* out);

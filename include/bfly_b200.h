@@ -84,6 +84,22 @@ int bfly_plan_prepare(bfly_plan* plan, uint32_t n, uint32_t batch);
  * buffers [batch][2n], n in [64, 4096]. */
 int bfly_plan_run_c2c(bfly_plan* plan, const float* in, float* out, uint32_t n, uint32_t batch);
 
+/* New: many synchronous host-to-host C2C requests in one call.  The reference transforms one
+ * request per call (Plan::run, butterfly.cpp:723-749: upload, launch, synchronise, download),
+ * so the copies of successive requests never overlap; here every request is validated first
+ * (-8 before any allocation or copy, any exec_c2c length, batch*2n fp32 per buffer), then their
+ * row chunks flow through an upload stream, the context stream and a download stream.  Pinned
+ * host buffers reach the bidirectional PCIe bandwidth. */
+typedef struct bfly_host_request {
+    const float* in;       /* [batch][2n] fp32, host */
+    float* out;            /* [batch][2n] fp32, host */
+    uint32_t n;
+    uint32_t batch;
+    int32_t direction;     /* -1 forward, +1 inverse */
+    float scale;
+} bfly_host_request;
+int bfly_plan_run_c2c_many(bfly_plan* plan, const bfly_host_request* reqs, size_t count);
+
 /* Replaces Plan::runR2C (plan.hpp:40, butterfly.cpp:753-806): [batch][n] -> [batch][n+2],
  * n in [128, 8192]. */
 int bfly_plan_run_r2c(bfly_plan* plan, const float* in, float* out, uint32_t n, uint32_t batch);

@@ -487,6 +487,31 @@ int main(int argc, char** argv) {
         CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
     }
 
+    {   // batched host round trip: equal to per-request device transforms; guards first
+        std::vector<float> a(2 * 64 * 3), b(2 * 96 * 2), c(2 * 128 * 4);
+        for (size_t i = 0; i < a.size(); ++i) a[i] = (float)std::sin(0.3 * i);
+        for (size_t i = 0; i < b.size(); ++i) b[i] = (float)std::cos(0.7 * i + 1);
+        for (size_t i = 0; i < c.size(); ++i) c[i] = (float)std::sin(1.1 * i * i);
+        std::vector<float> oa(a.size()), ob(b.size()), oc(c.size()), ra(a.size()), rb(b.size()), rc2(c.size());
+        const bfly::HostRequest reqs[] = {{a.data(), oa.data(), 64, 3, -1, 1.f},
+                                          {b.data(), ob.data(), 96, 2, -1, 1.f},
+                                          {c.data(), oc.data(), 128, 4, 1, 0.125f}};
+        CHECK(plan->runMany(reqs, 3) == 0);
+        CHECK(plan->execC2C(a.data(), ra.data(), 64, 3, -1, 1.f, nullptr) == 0);
+        CHECK(plan->execC2C(b.data(), rb.data(), 96, 2, -1, 1.f, nullptr) == 0);
+        CHECK(plan->execC2C(c.data(), rc2.data(), 128, 4, 1, 0.125f, nullptr) == 0);
+        CHECK(oa == ra && ob == rb && oc == rc2);
+        const int allocBefore = fake::allocations, copiesBefore = fake::copies, launchBefore = fake::launches;
+        CHECK(plan->runMany(nullptr, 1) == -8);
+        CHECK(plan->runMany(reqs, 0) == -8);
+        const bfly::HostRequest bad1[] = {reqs[0], {a.data(), oa.data(), 9000, 1, -1, 1.f}};
+        const bfly::HostRequest bad2[] = {reqs[0], {a.data(), oa.data(), 64, 1, 0, 1.f}};
+        const bfly::HostRequest bad3[] = {reqs[0], {nullptr, oa.data(), 64, 1, -1, 1.f}};
+        const bfly::HostRequest bad4[] = {reqs[0], {a.data(), oa.data(), 64, 0, -1, 1.f}};
+        for (const auto* bad : {bad1, bad2, bad3, bad4}) CHECK(plan->runMany(bad, 2) == -8);
+        CHECK(fake::allocations == allocBefore && fake::copies == copiesBefore && fake::launches == launchBefore);
+    }
+
     plan.reset();
     best.reset();
     cached.reset();
