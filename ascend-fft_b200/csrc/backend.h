@@ -24,6 +24,10 @@ int releaseHost(void* ptr);
 int copyH2D(void* dst, const void* src, size_t bytes, void* stream);
 int copyD2H(void* dst, const void* src, size_t bytes, void* stream);
 int streamSync(void* stream);
+// Opt kernel `fn` into `bytes` of dynamic shared memory on the current device (no-op at or below
+// the 48 KB default); done once per (device, kernel), thread-safe.
+int optInSharedMemory(const void* fn, int bytes);
+
 // Ordering between streams (events without timing).
 int eventCreate(void** event);
 int eventDestroy(void* event);

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <utility>
+#include <vector>
 
 namespace bfly {
 namespace backend {
@@ -104,21 +105,21 @@ size_t variantSmemBytes(int kind, uint32_t n, int e, int cta) {
 }
 
 // Raise the dynamic shared-memory limit once per kernel that needs more than 48 KB.
-// Opt a kernel into more than 48 KB of dynamic shared memory, once per (device, kernel).
-static int prepareEntry(const Entry* x) {
-    if (x->smem <= 48 * 1024) return 0;
+int optInSharedMemory(const void* fn, int bytes) {
+    if (bytes <= 48 * 1024) return 0;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return (int)cudaErrorInvalidDevice;
     static std::mutex mu;
-    static std::pair<int, const Entry*> done[1024];
-    static int ndone = 0;
+    static std::vector<std::pair<int, const void*>> done;
     std::lock_guard<std::mutex> lock(mu);
-    for (int i = 0; i < ndone; ++i)
-        if (done[i].first == device && done[i].second == x) return 0;
-    int e = rc(cudaFuncSetAttribute(x->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, x->smem));
-    if (!e && ndone < 1024) done[ndone++] = {device, x};
+    for (const auto& d : done)
+        if (d.first == device && d.second == fn) return 0;
+    const int e = rc(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (!e) done.push_back({device, fn});
     return e;
 }
+
+static int prepareEntry(const Entry* x) { return optInSharedMemory(x->fn, x->smem); }
 
 static unsigned gridFor(uint64_t batch, int rows) {
     return (unsigned)((batch + (uint64_t)rows - 1) / (uint64_t)rows);

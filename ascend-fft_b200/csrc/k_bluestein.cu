@@ -13,8 +13,6 @@
 // conjugate of the filter of h.
 #include <cuda_runtime.h>
 
-#include <atomic>
-
 #include "backend.h"
 #include "fft_kernels.cuh"
 
@@ -119,16 +117,7 @@ int launchBluesteinM(const void* in, void* out, uint32_t n, uint64_t batch, floa
     constexpr int ROWS = CTA / T;
     constexpr int SMEM = ROWS * dev::smem_stride<M, E, false>() * 8;
     auto* fn = dev::k_bluestein<M, E, ROWS, INV>;
-    if (SMEM > 48 * 1024) {
-        static std::atomic<uint64_t> devices{0};
-        int d = 0;
-        if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return (int)cudaErrorInvalidDevice;
-        if (!(devices.load() >> d & 1)) {
-            if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
-                return 1;
-            devices.fetch_or(1ull << d);
-        }
-    }
+    if (int e = optInSharedMemory((const void*)fn, SMEM)) return e;
     const uint64_t grid = (batch + ROWS - 1) / ROWS;
     if (grid > 0x7fffffffull) return (int)cudaErrorInvalidValue;
     fn<<<(unsigned)grid, CTA, SMEM, reinterpret_cast<cudaStream_t>(stream)>>>(

@@ -12,6 +12,9 @@
 // positions of the next pass (or, after the last pass, to global memory).
 // Twiddles between passes stay fp32 (the Stockham tables of the CUDA-core path, E = 16).
 // Inverse transforms use IDFT(x) = conj(DFT(conj x)).
+#include <atomic>
+
+#include "backend.h"
 #include "fft_kernels.cuh"
 #include "registry.cuh"
 #include "tcgen05.cuh"
@@ -247,17 +250,19 @@ template <int N, int SPLIT>
 static int launchTc(const void* in, void* out, uint64_t batch, bool inverse, float scale, const void* tw,
                     const void* table, void* stream) {
     constexpr int smem = dev::tcSmemBytes<N, SPLIT>();
-    static int resident = 0;   // CTAs resident on the whole device (persistent grid)
+    static std::atomic<int> residentOn[64];   // CTAs resident on each device (persistent grid)
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return (int)cudaErrorInvalidDevice;
+    int resident = residentOn[device].load();
     if (!resident) {
-        int dev = 0, sms = 0, perSm = 0;
-        if (cudaFuncSetAttribute(dev::k_c2c_tc<N, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-                cudaSuccess ||
-            cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        int sms = 0, perSm = 0;
+        if (optInSharedMemory((const void*)dev::k_c2c_tc<N, SPLIT>, smem) ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, dev::k_c2c_tc<N, SPLIT>, dev::kTcThreads, smem) !=
                 cudaSuccess)
             return 1;
         resident = sms * (perSm > 0 ? perSm : 1);
+        residentOn[device].store(resident);
     }
     constexpr int rows = dev::kTcThreads / (N / 16);
     const uint64_t groups = (batch + rows - 1) / rows;

@@ -4,6 +4,7 @@
 // same and a static stride over the tile space balances the grid; no atomics and no waits.
 // Inverse requests run the forward kernel on conj(x) and conjugate the result
 // (IDFT(x) = conj(DFT(conj x))), so one code path per length serves both directions.
+#include "backend.h"
 #include "fft_kernels.cuh"
 #include "ragged.h"
 #include "tma.cuh"
@@ -288,13 +289,7 @@ int launchRaggedStaged(const void* entries, int count, uint64_t totalTiles, int 
 
 int launchRaggedFlat(const void* entries, int count, const void* tileMap, uint64_t totalTiles, void* stream) {
     if (count <= 0 || totalTiles == 0) return 0;
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(dev::k_ragged_flat, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 raggedSmemBytes()) != cudaSuccess)
-            return 1;
-        attr = true;
-    }
+    if (int e = optInSharedMemory((const void*)dev::k_ragged_flat, raggedSmemBytes())) return e;
     const auto* es = static_cast<const RaggedEntry*>(entries);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     for (uint64_t base = 0; base < totalTiles; base += 0x7fffffffull) {
