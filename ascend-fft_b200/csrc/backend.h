@@ -84,6 +84,14 @@ int launchLongCluster(const void* in, void* out, uint32_t n, uint64_t batch, boo
                       const void* tw1, const void* tw2, const void* tlo, const void* thi, int cta, void* stream);
 int longClusterStatus(unsigned* status, bool clear);   // device error word of the cluster kernel; 0 on success
 
+// C2C of n = A*B by the prime-factor (Good-Thomas) mapping: A in {3, 5, 9, 15}, B a power of two
+// >= 16, n <= kPfaMaxN.  pfaSplit gives (A, B) or false; twB = Stockham table (B, 16), wA =
+// W_A^m, m < A (linear table of A entries for length A).
+constexpr uint32_t kPfaMaxN = 12288;
+bool pfaSplit(uint32_t n, uint32_t* a, uint32_t* b);
+int launchPfa(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale, const void* twB,
+              const void* wA, void* stream);
+
 // Any-length C2C (Bluestein), n in [2, kBluesteinMaxN], in one kernel per padded length M =
 // bluesteinM(n) (power of two >= 2n-1, >= 64).  Tables per n: chirp (n float2), filter (M
 // float2), built in FP64 on the device with an M-double2 scratch; tw = Stockham table (M, 16).

@@ -356,6 +356,7 @@ struct Plan::Impl {
         void* filt = nullptr;    // FFT_M of the padded conj(c) sequence, / M
     };
     std::map<uint32_t, Chirp> bluestein;   // non-power-of-two n -> Bluestein tables
+    std::map<uint32_t, void*> dftSmall;    // A -> W_A^m, m < A (prime-factor kernels)
 };
 
 Plan::Plan(Candidate c) : cand_(std::move(c)) {}
@@ -378,6 +379,8 @@ Plan::~Plan() {
         if (e) backend::eventDestroy(e);
     for (void* t : impl_->tcTable)
         if (t) backend::release(t);
+    for (auto& kv : impl_->dftSmall)
+        if (kv.second) backend::release(kv.second);
     for (auto& kv : impl_->bluestein) {
         if (kv.second.chirp) backend::release(kv.second.chirp);
         if (kv.second.filt) backend::release(kv.second.filt);
@@ -402,8 +405,11 @@ static int ensureBuf(void** p, size_t* cap, size_t bytes) {
 bool Plan::validShape(uint32_t n, uint32_t batch, int kind) const {
     if (!impl_ || batch == 0) return false;
     // lengths outside the power-of-two kernels (non-powers of two, and 2..16) only through the
-    // device-pointer C2C entry (Bluestein)
-    if (!pow2(n) || (kind == kExecC2C && n < kMinN)) return kind == kExecC2C && backend::bluesteinM(n) != 0;
+    // device-pointer C2C entry (prime-factor kernel for A*2^k, else Bluestein)
+    if (!pow2(n) || (kind == kExecC2C && n < kMinN)) {
+        uint32_t a = 0, b = 0;
+        return kind == kExecC2C && (backend::bluesteinM(n) != 0 || backend::pfaSplit(n, &a, &b));
+    }
     const bool offsetGuard = kind == kRunC2C || kind == kRunR2C || kind == kRunC2R ||
                              kind == kRunLong || kind == kMeasure;
     switch (kind) {
@@ -512,6 +518,20 @@ int Plan::prepareLong(uint32_t n) {
     return 0;
 }
 
+int Plan::preparePfa(uint32_t n) {
+    uint32_t a = 0, b = 0;
+    if (!backend::pfaSplit(n, &a, &b) || prepareC2C(b, kColsE)) return -1;
+    if (impl_->dftSmall.count(a)) return 0;
+    void* w = nullptr;
+    if (backend::alloc(&w, (size_t)a * 8)) return -1;
+    if (backend::buildLinearTwiddles(w, (int)a, 1, a, stream_) || backend::streamSync(stream_)) {
+        backend::release(w);
+        return -1;
+    }
+    impl_->dftSmall[a] = w;
+    return 0;
+}
+
 int Plan::prepareBluestein(uint32_t n) {
     const uint32_t M = backend::bluesteinM(n);
     if (!M || prepareC2C(M, kColsE)) return -1;
@@ -563,6 +583,13 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
     if (!validShape(n, (uint32_t)batch, kExecC2C)) return -8;
     void* s = stream;   // NULL is the CUDA default stream
     const bool inv = direction > 0;
+    uint32_t pa = 0, pb = 0;
+    if (!pow2(n) && backend::pfaSplit(n, &pa, &pb)) {   // n = A * 2^k: prime-factor kernel
+        if (preparePfa(n)) return -2;
+        if (backend::launchPfa(dIn, dOut, n, batch, inv, scale, impl_->twC2C[{pb, kColsE}], impl_->dftSmall[pa], s))
+            return -5;
+        return 0;
+    }
     if (!pow2(n) || n < kMinN) {   // Bluestein: one kernel on the padded power-of-two length
         if (prepareBluestein(n)) return -2;
         const auto& t = impl_->bluestein[n];

@@ -204,8 +204,9 @@ public:
     // synchronisation, no host<->device copies.
     //   direction -1 forward, +1 inverse; scale multiplies the output.
     //   n in [32, 16384] single pass, [8192, 65536] four-step (workspace grown on demand);
-    //   any other n in [2, 8192] (non-powers of two, and 2..16) by Bluestein's algorithm in
-    //   one kernel (the first call for a length builds its chirp and filter tables).
+    //   n = A * 2^k (A in {3, 5, 9, 15}, 2^k >= 16, n <= 12288) by the prime-factor mapping in
+    //   one kernel; any other n in [2, 8192] (non-powers of two, and 2..16) by Bluestein's
+    //   algorithm in one kernel (the first call for a length builds its chirp and filter tables).
     int execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                 float scale, void* stream);
     // 2-D C2C over [batch][ny][nx] complex, rows of nx contiguous: nx-point row transforms
@@ -258,6 +259,7 @@ private:
     int prepareReal(uint32_t n);
     int prepareLong(uint32_t n);
     int prepareBluestein(uint32_t n);
+    int preparePfa(uint32_t n);
     int resolve(int kind, uint32_t n, int* e, int* cta) const;
     int execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                     float scale, void* stream, void* work);

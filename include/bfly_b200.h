@@ -127,8 +127,9 @@ int bfly_plan_run_c2c_long(bfly_plan* plan, const float* in, float* out, uint32_
  * synchronising.  The first call for a length builds
  * its twiddle tables (and the four-step workspace) and synchronises the context stream once;
  * make it before any stream capture. */
-/* C2C, power-of-two n in [32, 65536], or any n in [2, 8192] (non-powers of two and 2..16 by
- * Bluestein's algorithm in one kernel; the reference supports powers of two only,
+/* C2C, power-of-two n in [32, 65536], n = A*2^k (A in {3, 5, 9, 15}, 2^k >= 16, n <= 12288) by
+ * the prime-factor mapping in one kernel, or any n in [2, 8192] (the other non-powers of two
+ * and 2..16 by Bluestein's algorithm in one kernel; the reference supports powers of two only,
  * docs/reference/support.md:14); direction -1 forward / +1 inverse; output multiplied by
  * scale. */
 int bfly_plan_exec_c2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,

@@ -145,6 +145,25 @@ int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
     return 0;
 }
 
+bool pfaSplit(uint32_t n, uint32_t* a, uint32_t* b) {
+    *a = *b = 0;
+    for (uint32_t A : {3u, 5u, 9u, 15u})
+        if (n % A == 0 && n / A >= 16 && !((n / A) & (n / A - 1)) && n <= kPfaMaxN) {
+            *a = A;
+            *b = n / A;
+        }
+    return *a != 0;
+}
+int launchPfa(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale, const void*,
+              const void*, void*) {
+    uint32_t a = 0, b = 0;
+    if (!pfaSplit(n, &a, &b)) return 1;
+    if (int r = launch()) return r;
+    for (uint64_t r = 0; r < batch; ++r)
+        dft((const float*)in + r * 2 * n, (float*)out + r * 2 * n, n, inverse ? 1 : -1, scale);
+    return 0;
+}
+
 uint32_t bluesteinM(uint32_t n) {
     if (n < 2 || n > kBluesteinMaxN) return 0;
     uint32_t m = 64;
