@@ -16,12 +16,98 @@
 namespace bfly {
 namespace dev {
 
+// ------------------------------------------------------------------ small odd DFTs
+// Forward sign exp(-2*pi*i/A); INV flips it.  Constants are cos/sin of 2*pi/3, 2*pi/5, 4*pi/5.
+__device__ __forceinline__ float2 mul_i(float2 a, bool neg) {   // -i*a (neg) or +i*a
+    return neg ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft3(float2& x0, float2& x1, float2& x2) {
+    constexpr float kS3 = 0.866025403784438647f;   // sin(2*pi/3)
+    const float2 t1 = cadd(x1, x2);
+    const float2 t2 = make_float2(x1.x - x2.x, x1.y - x2.y);
+    const float2 m = make_float2(x0.x - 0.5f * t1.x, x0.y - 0.5f * t1.y);
+    const float2 r = mul_i(make_float2(kS3 * t2.x, kS3 * t2.y), !INV);
+    x0 = cadd(x0, t1);
+    x1 = cadd(m, r);
+    x2 = make_float2(m.x - r.x, m.y - r.y);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft5(float2& x0, float2& x1, float2& x2, float2& x3, float2& x4) {
+    constexpr float kC1 = 0.309016994374947424f, kC2 = -0.809016994374947424f;   // cos(2pi/5), cos(4pi/5)
+    constexpr float kS1 = 0.951056516295153572f, kS2 = 0.587785252292473129f;    // sin(2pi/5), sin(4pi/5)
+    const float2 t1 = cadd(x1, x4), t2 = cadd(x2, x3);
+    const float2 t3 = make_float2(x1.x - x4.x, x1.y - x4.y), t4 = make_float2(x2.x - x3.x, x2.y - x3.y);
+    const float2 a1 = make_float2(x0.x + kC1 * t1.x + kC2 * t2.x, x0.y + kC1 * t1.y + kC2 * t2.y);
+    const float2 a2 = make_float2(x0.x + kC2 * t1.x + kC1 * t2.x, x0.y + kC2 * t1.y + kC1 * t2.y);
+    const float2 b1 = mul_i(make_float2(kS1 * t3.x + kS2 * t4.x, kS1 * t3.y + kS2 * t4.y), !INV);
+    const float2 b2 = mul_i(make_float2(kS2 * t3.x - kS1 * t4.x, kS2 * t3.y - kS1 * t4.y), !INV);
+    x0 = cadd(x0, cadd(t1, t2));
+    x1 = cadd(a1, b1);
+    x4 = make_float2(a1.x - b1.x, a1.y - b1.y);
+    x2 = cadd(a2, b2);
+    x3 = make_float2(a2.x - b2.x, a2.y - b2.y);
+}
+
+// In-place A-point DFT of x (natural order in and out); w = W_A^m, m < A (used by A = 9).
+template <int A, bool INV>
+__device__ __forceinline__ void dft_odd(float2 (&x)[A], const float2 (&w)[A]) {
+    if constexpr (A == 3) {
+        dft3<INV>(x[0], x[1], x[2]);
+    } else if constexpr (A == 5) {
+        dft5<INV>(x[0], x[1], x[2], x[3], x[4]);
+    } else if constexpr (A == 9) {   // 3 x 3 Cooley-Tukey: j = 3 j1 + j2, k = k1 + 3 k2
+#pragma unroll
+        for (int j2 = 0; j2 < 3; ++j2) dft3<INV>(x[j2], x[3 + j2], x[6 + j2]);   // x[3 k1 + j2] = y[j2][k1]
+#pragma unroll
+        for (int j2 = 1; j2 < 3; ++j2)
+#pragma unroll
+            for (int k1 = 1; k1 < 3; ++k1) x[3 * k1 + j2] = cmul<INV>(x[3 * k1 + j2], w[j2 * k1]);
+        float2 y[9];
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) {
+            float2 a = x[3 * k1], b = x[3 * k1 + 1], c = x[3 * k1 + 2];
+            dft3<INV>(a, b, c);
+            y[k1] = a;
+            y[k1 + 3] = b;
+            y[k1 + 6] = c;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) x[k] = y[k];
+    } else {   // A == 15: 3 x 5 Good-Thomas, j <-> (j mod 3, j mod 5), k = (5 k1 + 3 k2) mod 15
+        static_assert(A == 15, "small odd DFTs: 3, 5, 9, 15");
+        float2 z[15];   // z[5 k1 + j2]
+#pragma unroll
+        for (int j2 = 0; j2 < 5; ++j2) {
+            // j = (10 j1 + 6 j2) mod 15 has j mod 3 = j1 and j mod 5 = j2
+            float2 a = x[(6 * j2) % 15], b = x[(10 + 6 * j2) % 15], c = x[(20 + 6 * j2) % 15];
+            dft3<INV>(a, b, c);
+            z[j2] = a;
+            z[5 + j2] = b;
+            z[10 + j2] = c;
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) {
+            float2* r = z + 5 * k1;
+            dft5<INV>(r[0], r[1], r[2], r[3], r[4]);
+#pragma unroll
+            for (int k2 = 0; k2 < 5; ++k2) x[(5 * k1 + 3 * k2) % 15] = r[k2];
+        }
+    }
+}
+
 template <int A, int B>
 struct Pfa {
     static constexpr int N = A * B, E = 16;
     static constexpr int TR = B / E;                      // threads per B-point sub-row
     static constexpr int T = A * TR;                      // threads per n-point row
-    static constexpr int SB = smem_stride<B, E, false>(); // sub-row stride (padded exchange)
+    // Sub-row stride.  The load scatter sends lane i to bank pair (i + (i mod A)*SB) mod 16, a
+    // permutation of the half-warp when SB is a multiple of 16; that is safe for the B-point
+    // passes once a half-warp lies inside one sub-row (TR >= 16).  Narrower sub-rows keep the
+    // exchange layout's own stride rule.
+    static constexpr int SB = TR >= 16 ? (smem_stride<B, E, false>() + 15) / 16 * 16 : smem_stride<B, E, false>();
     static constexpr int NAT = spad(N - 1) + 1;           // natural-order staging extent
     static constexpr int ROWBUF = (A * SB > NAT ? A * SB : NAT) | 1;
     static constexpr int CTA = T < 256 ? (256 / T) * T : T;
@@ -32,7 +118,7 @@ struct Pfa {
 };
 
 template <int A, int B, bool INV>
-__global__ void __launch_bounds__(Pfa<A, B>::CTA)
+__global__ void __launch_bounds__(Pfa<A, B>::CTA, min_blocks_64regs(Pfa<A, B>::CTA))
 k_pfa(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ twB,
       const float2* __restrict__ wA, uint64_t batch, float scale) {
     using P = Pfa<A, B>;
@@ -83,13 +169,9 @@ k_pfa(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     for (int c = 0; c < P::COLS; ++c) {
         const int k2 = tid + c * T;
         if (k2 < B) {
+            dft_odd<A, INV>(col[c], w);
 #pragma unroll
-            for (int k1 = 0; k1 < A; ++k1) {
-                float2 acc = col[c][0];
-#pragma unroll
-                for (int j1 = 1; j1 < A; ++j1) acc = cadd(acc, cmul<INV>(col[c][j1], w[(j1 * k1) % A]));
-                buf[spad((B * k1 + A * k2) % N)] = acc;
-            }
+            for (int k1 = 0; k1 < A; ++k1) buf[spad((B * k1 + A * k2) % N)] = col[c][k1];
         }
     }
     __syncthreads();
