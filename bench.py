@@ -287,7 +287,7 @@ def extra_measurements(dev, stream):
     """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores vs fp32 at the
     largest power-of-16 grid points; long C2C forward + backward (batch*n = 2^26; single pass up
     to n = 16384, four-step above); 2-D C2C at the reference's planned 2-D / range-Doppler shapes
-    and transforms along a middle axis; any-length C2C (Bluestein); STFT; real transforms
+    and transforms along a middle axis; non-power-of-two C2C (prime-factor, Bluestein); STFT; real transforms
     forward + adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
     events on `stream` around one replay of a CUDA graph holding 20 launches (after 3 warm-up
     launches), and the error against FP64 on sampled rows."""
@@ -390,9 +390,10 @@ def extra_measurements(dev, stream):
             "gbs": round(16 * n * outer * inner / ms / 1e6, 1),
             "frac": round(16 * n * outer * inner / ms / 1e6 / peak, 4), "rel_l2": err, "passes": 1}
         del x, y
-    # ---- any-length C2C (Bluestein, one kernel), batch * n ~ 2^25
+    # ---- non-power-of-two C2C, batch * n ~ 2^25: prime-factor kernel (n = A * 2^k) and
+    # Bluestein (other lengths), one kernel each
     out["c2c_any_length"] = {}
-    for n in (1000, 3000, 8191):
+    for n in (1536, 1920, 6144, 1000, 3000, 8191):
         b = (1 << 25) // n
         g = torch.Generator(device=dev).manual_seed(n)
         x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
@@ -400,8 +401,10 @@ def extra_measurements(dev, stream):
         plan = bfly.plan_for(dev, n)
         ms = timed(lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh))
         gbs = 16 * n * b / ms / 1e6
-        out["c2c_any_length"][f"n{n}_b{b}"] = {"gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
-                                               "rel_l2": rel(y, x), "padded_length": 1 << (2 * n - 2).bit_length()}
+        pfa = any(n % a == 0 and (n // a) & (n // a - 1) == 0 and n // a >= 16 for a in (3, 5, 9, 15))
+        out["c2c_any_length"][f"n{n}_b{b}"] = {
+            "gbs": round(gbs, 1), "frac": round(gbs / peak, 4), "rel_l2": rel(y, x),
+            "kernel": "prime-factor" if pfa else f"bluestein (padded length {1 << (2 * n - 2).bit_length()})"}
         del x, y
     # ---- STFT (frame gather + Hann window + one-sided transform in one kernel), 4 signals of
     # 2^24 samples, centred; bytes counted per frame as the reference's dense-frame R2C proxy
