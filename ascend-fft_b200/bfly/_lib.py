@@ -44,6 +44,10 @@ SIGNATURES = {
                                            C.c_int, C.c_float, C.c_void_p]),
     "bfly_plan_exec_c2c_2d_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                               C.c_uint64, C.c_int, C.c_float, C.c_void_p]),
+    "bfly_plan_exec_r2c_2d_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                              C.c_uint64, C.c_float, C.c_void_p]),
+    "bfly_plan_exec_c2r_2d_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                              C.c_uint64, C.c_float, C.c_void_p]),
     "bfly_plan_exec_c2c_axis_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
                                                 C.c_uint64, C.c_int, C.c_float, C.c_void_p]),
     "bfly_plan_exec_stft_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,

@@ -165,6 +165,16 @@ class Plan:
         return self._lib.bfly_plan_exec_c2c_2d_async(self._h, d_in, d_out, ny, nx, batch, direction,
                                                      scale, stream or None)
 
+    def exec_r2c_2d(self, d_in: int, d_out: int, ny: int, nx: int, batch: int, scale: float = 1.0,
+                    stream: int = 0) -> int:
+        """[batch][ny][nx] float32 -> [batch][ny][nx/2+1] complex64 (rfft2), times scale."""
+        return self._lib.bfly_plan_exec_r2c_2d_async(self._h, d_in, d_out, ny, nx, batch, scale, stream or None)
+
+    def exec_c2r_2d(self, d_in: int, d_out: int, ny: int, nx: int, batch: int, scale: float = 1.0,
+                    stream: int = 0) -> int:
+        """[batch][ny][nx/2+1] complex64 -> [batch][ny][nx] float32 (irfft2 times ny*nx*scale)."""
+        return self._lib.bfly_plan_exec_c2r_2d_async(self._h, d_in, d_out, ny, nx, batch, scale, stream or None)
+
     def exec_c2c_axis(self, d_in: int, d_out: int, n: int, outer: int, inner: int,
                       direction: int = -1, scale: float = 1.0, stream: int = 0) -> int:
         """C2C along the middle axis of a contiguous [outer][n][inner] complex64 array."""

@@ -6,6 +6,8 @@ hand-written adjoints behind torch.autograd.Function:
                             over the contiguous [outer][n][inner] view)
     fft2(x) / ifft2(x)      complex64 [..., ny, nx]: row pass (nx as fft) + column pass
                             (ny in 32..4096)
+    rfft2(x) / irfft2(X)    float32 [..., ny, nx] <-> complex64 [..., ny, nx/2+1] (row R2C + column
+                            pass; ny in 32..4096)
     stft(x, n_fft, ...)     float32 [..., L] -> complex64 [..., n_fft/2+1, frames], torch.stft's
                             arguments and defaults (centred reflect padding, hop n_fft/4); framing,
                             window and one-sided transform in one kernel
@@ -360,6 +362,56 @@ def stft(x: torch.Tensor, n_fft: int, hop_length: int | None = None, window: tor
     return y.reshape(*lead, y.shape[-2], y.shape[-1]).transpose(-1, -2)
 
 
+class _RFFT2(torch.autograd.Function):
+    """rfft2 = column FFT o row R2C; adjoint = row R2C^T (weighted C2R) o conjugate column FFT."""
+
+    @staticmethod
+    def forward(ctx, x, scale):
+        _need_cuda(x, torch.float32, "rfft2")
+        x = x.contiguous()
+        ny, nx = x.shape[-2], x.shape[-1]
+        batch = x.numel() // (ny * nx) if ny * nx else 0
+        y = torch.empty(*x.shape[:-1], nx // 2 + 1, dtype=torch.complex64, device=x.device)
+        ctx.scale, ctx.nx = scale, nx
+        if batch == 0:
+            return y
+        rc = plan_for(x.device, nx, "real").exec_r2c_2d(x.data_ptr(), y.data_ptr(), ny, nx, batch, scale, _stream(x))
+        if rc:
+            raise BflyError(f"exec_r2c_2d(ny={ny}, nx={nx}, batch={batch})", rc)
+        return y
+
+    @staticmethod
+    def backward(ctx, g):
+        gc = c2c_axis(g.contiguous(), -2, 1, 1.0)
+        return c2r(gc, ctx.nx, 1.0, 0.5, ctx.scale), None
+
+
+class _IRFFT2(torch.autograd.Function):
+    """irfft2 = row C2R o inverse column FFT; adjoint = forward column FFT o row C2R^T (weighted R2C)."""
+
+    @staticmethod
+    def forward(ctx, X, nx, scale):
+        _need_cuda(X, torch.complex64, "irfft2")
+        X = X.contiguous()
+        ny = X.shape[-2]
+        if X.shape[-1] != nx // 2 + 1:
+            raise ValueError(f"irfft2: last dimension {X.shape[-1]} != nx/2+1 = {nx // 2 + 1}")
+        batch = X.numel() // (ny * X.shape[-1]) if X.numel() else 0
+        y = torch.empty(*X.shape[:-1], nx, dtype=torch.float32, device=X.device)
+        ctx.scale = scale
+        if batch == 0:
+            return y
+        rc = plan_for(X.device, nx, "real").exec_c2r_2d(X.data_ptr(), y.data_ptr(), ny, nx, batch, scale, _stream(X))
+        if rc:
+            raise BflyError(f"exec_c2r_2d(ny={ny}, nx={nx}, batch={batch})", rc)
+        return y
+
+    @staticmethod
+    def backward(ctx, g):
+        c = ctx.scale
+        return c2c_axis(r2c(g.contiguous(), c, 2.0 * c), -2, -1, 1.0), None, None
+
+
 def _need_2d(x: torch.Tensor, what: str):
     if x.dim() < 2:
         raise ValueError(f"{what}: input needs at least two dimensions")
@@ -374,6 +426,23 @@ def fft2(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:
 def ifft2(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:
     _need_2d(x, "ifft2")
     return _FFT2.apply(x, 1, _scale(norm, x.shape[-2] * x.shape[-1], False))
+
+
+def rfft2(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:
+    """torch.fft.rfft2 over the last two dimensions: float32 [..., ny, nx] -> [..., ny, nx/2+1]."""
+    _need_2d(x, "rfft2")
+    return _RFFT2.apply(x, _scale(norm, x.shape[-2] * x.shape[-1], True))
+
+
+def irfft2(X: torch.Tensor, s: tuple | None = None, norm: str | None = None) -> torch.Tensor:
+    """torch.fft.irfft2 over the last two dimensions; s = (ny, nx) output size (default
+    (X.shape[-2], 2*(X.shape[-1]-1)))."""
+    _need_2d(X, "irfft2")
+    ny = X.shape[-2]
+    nx = s[-1] if s is not None else 2 * (X.shape[-1] - 1)
+    if s is not None and s[-2] != ny:
+        raise ValueError("irfft2: s[-2] must equal X.shape[-2] (no cropping or padding)")
+    return _IRFFT2.apply(X, nx, _scale(norm, ny * nx, False))
 
 
 def rfft(x: torch.Tensor, norm: str | None = None) -> torch.Tensor:

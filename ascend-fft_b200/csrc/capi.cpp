@@ -182,6 +182,18 @@ int bfly_plan_exec_c2c_2d_async(bfly_plan* plan, const void* d_in, void* d_out, 
     return p.execC2C2D(d_in, d_out, ny, nx, batch, direction, scale, stream);
 }
 
+int bfly_plan_exec_r2c_2d_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t ny,
+                                uint32_t nx, uint64_t batch, float scale, void* stream) {
+    PLAN_OR_FAIL();
+    return p.execR2C2D(d_in, d_out, ny, nx, batch, scale, stream);
+}
+
+int bfly_plan_exec_c2r_2d_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t ny,
+                                uint32_t nx, uint64_t batch, float scale, void* stream) {
+    PLAN_OR_FAIL();
+    return p.execC2R2D(d_in, d_out, ny, nx, batch, scale, stream);
+}
+
 int bfly_plan_exec_c2c_axis_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                                   uint64_t outer, uint64_t inner, int direction, float scale,
                                   void* stream) {

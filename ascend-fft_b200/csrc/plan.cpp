@@ -350,6 +350,8 @@ struct Plan::Impl {
     backend::Timer* timer = nullptr;
     void* aux[2] = {nullptr, nullptr};   // upload / download streams of the pipelined host round trip
     void* ev[2] = {nullptr, nullptr};    // chunk uploaded / chunk transformed
+    void* devHalf = nullptr;             // column-transformed half spectrum of execC2R2D
+    size_t devHalfCap = 0;
     void* tcTable[4] = {nullptr, nullptr, nullptr, nullptr};   // split DFT-16 operand per term count
     struct Chirp {
         void* chirp = nullptr;   // c[j] = exp(-i*pi*j^2/n), j < n
@@ -372,6 +374,7 @@ Plan::~Plan() {
     if (impl_->devIn) backend::release(impl_->devIn);
     if (impl_->devOut) backend::release(impl_->devOut);
     if (impl_->devWork) backend::release(impl_->devWork);
+    if (impl_->devHalf) backend::release(impl_->devHalf);
     backend::timerDestroy(impl_->timer);
     for (void* st : impl_->aux)
         if (st) backend::streamDestroy(st);
@@ -731,6 +734,25 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
                            sEdge, sInt, outScale, stream))
         return -5;
     return 0;
+}
+
+int Plan::execR2C2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch, float scale,
+                    void* stream) {
+    if (!dIn || !dOut || batch == 0 || !pow2(ny) || !backend::hasCols(ny)) return -8;
+    if (batch * ny > 0xFFFFFFFFull) return -8;
+    const uint32_t half = nx / 2 + 1;
+    if (int r = execR2C(dIn, dOut, nx, batch * ny, 1.0f, 1.0f, stream)) return r;
+    return execCols(dOut, dOut, ny, batch, half, half, false, scale, stream);
+}
+
+int Plan::execC2R2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch, float scale,
+                    void* stream) {
+    if (!dIn || !dOut || batch == 0 || !pow2(ny) || !backend::hasCols(ny)) return -8;
+    if (batch * ny > 0xFFFFFFFFull || !validShape(nx, (uint32_t)(batch * ny), kExecC2R)) return -8;
+    const uint32_t half = nx / 2 + 1;
+    if (ensureBuf(&impl_->devHalf, &impl_->devHalfCap, (size_t)batch * ny * half * 8)) return -3;
+    if (int r = execCols(dIn, impl_->devHalf, ny, batch, half, half, true, 1.0f, stream)) return r;
+    return execC2R(impl_->devHalf, dOut, nx, batch * ny, 1.0f, 1.0f, scale, stream);
 }
 
 // Body of the synchronous host-pointer entry points: upload, enqueue, synchronise, download.

@@ -214,6 +214,14 @@ public:
     // (ny in [32, 4096]); scale applied once.  batch * ny <= 2^32 - 1.
     int execC2C2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch,
                   int direction, float scale, void* stream);
+    // 2-D real transforms over [batch][ny][nx] real <-> [batch][ny][nx/2+1] complex (numpy.fft
+    // rfft2 / irfft2 layouts), nx as execR2C / execC2R, ny in [32, 4096] (power of two):
+    //   execR2C2D: R2C rows into dOut, column transforms in place; output times scale.
+    //   execC2R2D: inverse column transforms of dIn into a plan-owned buffer (dIn is not
+    //   modified), then C2R rows; output times scale (1/(ny*nx) = numpy.fft.irfft2).  Imaginary
+    //   parts of each row's bins 0 and nx/2 after the column pass are ignored, as in execC2R.
+    int execR2C2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch, float scale, void* stream);
+    int execC2R2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch, float scale, void* stream);
     // C2C along the middle axis of a contiguous [outer][n][inner] complex array: element i of
     // transform (o, c) at (o*n + i)*inner + c.  inner == 1 is execC2C (n in [32, 65536]);
     // inner > 1 runs the column kernel (n in [32, 4096]).  dIn == dOut allowed.

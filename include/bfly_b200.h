@@ -142,6 +142,15 @@ int bfly_plan_exec_c2c_async(bfly_plan* plan, const void* d_in, void* d_out, uin
 int bfly_plan_exec_c2c_2d_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t ny,
                                 uint32_t nx, uint64_t batch, int direction, float scale,
                                 void* stream);
+/* New: 2-D real transforms (numpy.fft.rfft2 / irfft2 layouts): [batch][ny][nx] fp32 <->
+ * [batch][ny][nx/2+1] complex64; nx in the R2C / C2R envelope, ny in [32, 4096] (power of two);
+ * output times scale.  r2c_2d: R2C rows then column transforms in place in d_out; c2r_2d:
+ * inverse column transforms into a plan-owned buffer (d_in unchanged), then C2R rows.  The
+ * reference has no 2-D transform (docs/reference/support.md:14). */
+int bfly_plan_exec_r2c_2d_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t ny,
+                                uint32_t nx, uint64_t batch, float scale, void* stream);
+int bfly_plan_exec_c2r_2d_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t ny,
+                                uint32_t nx, uint64_t batch, float scale, void* stream);
 /* New: C2C along the middle axis of a contiguous [outer][n][inner] complex array (element i
  * of transform (o, c) at (o*n + i)*inner + c): inner == 1 is exec_c2c; inner > 1 needs n in
  * [32, 4096].  d_in == d_out allowed.  The reference supports contiguous rows only

@@ -439,6 +439,12 @@ int main(int argc, char** argv) {
         CHECK(plan->execC2CAxis(d, d, 32, 1, 0, -1, 1.f, nullptr) == -8);
         CHECK(plan->execC2CAxis(d, d, 8192, 1, 3, -1, 1.f, nullptr) == -8);   // strided n above 4096
         CHECK(plan->execC2CAxis(d, d, 100, 1, 3, -1, 1.f, nullptr) == -8);
+        CHECK(plan->execR2C2D(nullptr, d, 32, 64, 1, 1.f, nullptr) == -8);
+        CHECK(plan->execR2C2D(d, d, 48, 64, 1, 1.f, nullptr) == -8);        // ny not a power of two
+        CHECK(plan->execR2C2D(d, d, 32, 96, 1, 1.f, nullptr) == -8);        // nx outside R2C
+        CHECK(plan->execC2R2D(d, d, 8192, 64, 1, 1.f, nullptr) == -8);      // ny above 4096
+        CHECK(plan->execC2R2D(d, d, 32, 16384, 1, 1.f, nullptr) == -8);     // nx outside C2R
+        CHECK(plan->execC2R2D(d, d, 32, 64, 0, 1.f, nullptr) == -8);
         CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
     }
 

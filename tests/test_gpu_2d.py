@@ -122,3 +122,49 @@ def test_unsupported_shapes_raise(cuda):
         bfly.fft(_cplx((8192, 4), 1, cuda), dim=0)    # strided n above 4096
     with pytest.raises(ValueError):
         bfly.fft2(torch.zeros(64, dtype=torch.complex64, device=cuda))
+
+
+@pytest.mark.parametrize("ny,nx", [(32, 64), (256, 256), (1024, 128), (64, 8192), (4096, 64)])
+def test_real_2d_matches_fp64(plan, cuda, ny, nx):
+    """rfft2 / irfft2 layouts of numpy: [b][ny][nx] real <-> [b][ny][nx/2+1] complex."""
+    import torch
+    batch = 2
+    g = torch.Generator(device=cuda).manual_seed(ny + nx)
+    x = torch.rand(batch, ny, nx, device=cuda, generator=g) * 2 - 1
+    X = torch.empty(batch, ny, nx // 2 + 1, dtype=torch.complex64, device=cuda)
+    assert plan.exec_r2c_2d(x.data_ptr(), X.data_ptr(), ny, nx, batch, 1.0, 0) == 0
+    torch.cuda.synchronize()
+    ref = np.fft.rfft2(x.cpu().numpy().astype(np.float64))
+    assert _rel_mats(X.cpu().numpy(), ref) <= 2e-6
+    Xc = X.clone()
+    back = torch.empty_like(x)
+    assert plan.exec_c2r_2d(X.data_ptr(), back.data_ptr(), ny, nx, batch, 1.0 / (ny * nx), 0) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(X, Xc)                       # the input half spectrum is not modified
+    refb = np.fft.irfft2(ref, s=(ny, nx))
+    d = np.linalg.norm((back.cpu().numpy() - refb).reshape(batch, -1), axis=-1)
+    assert float((d / np.linalg.norm(refb.reshape(batch, -1), axis=-1)).max()) <= 3e-6
+
+
+def test_real_2d_torch_layer_and_autograd(cuda):
+    import torch
+    import bfly
+    g = torch.Generator(device=cuda).manual_seed(12)
+    x0 = torch.randn(3, 64, 128, device=cuda, generator=g)
+    for norm in (None, "ortho", "forward"):
+        ref = torch.fft.rfft2(x0, norm=norm)
+        got = bfly.rfft2(x0, norm=norm)
+        assert (torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)).item() <= 3e-6
+        back = bfly.irfft2(got, norm=norm)
+        assert (torch.linalg.vector_norm(back - x0) / torch.linalg.vector_norm(x0)).item() <= 3e-6
+    w = torch.rand(3, 64, 65, device=cuda, generator=g)
+    xa, xb = x0.clone().requires_grad_(True), x0.clone().requires_grad_(True)
+    (w * bfly.rfft2(xa, norm="ortho").abs() ** 2).sum().backward()
+    (w * torch.fft.rfft2(xb, norm="ortho").abs() ** 2).sum().backward()
+    assert (torch.linalg.vector_norm(xa.grad - xb.grad) / torch.linalg.vector_norm(xb.grad)).item() <= 1e-5
+    X0 = torch.fft.rfft2(x0)
+    wr = torch.rand(3, 64, 128, device=cuda, generator=g)
+    Xa, Xb = X0.clone().requires_grad_(True), X0.clone().requires_grad_(True)
+    (wr * bfly.irfft2(Xa) ** 2).sum().backward()
+    (wr * torch.fft.irfft2(Xb) ** 2).sum().backward()
+    assert (torch.linalg.vector_norm(Xa.grad - Xb.grad) / torch.linalg.vector_norm(Xb.grad)).item() <= 1e-5
