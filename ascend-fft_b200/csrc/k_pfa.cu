@@ -98,6 +98,13 @@ __device__ __forceinline__ void dft_odd(float2 (&x)[A], const float2 (&w)[A]) {
     }
 }
 
+// x with (a * x) mod m == 1 (gcd(a, m) = 1), at compile time.
+constexpr int mod_inverse(int a, int m) {
+    for (int x = 1; x < m; ++x)
+        if ((a * x) % m == 1) return x;
+    return 1;
+}
+
 template <int A, int B>
 struct Pfa {
     static constexpr int N = A * B, E = 16;
@@ -108,11 +115,12 @@ struct Pfa {
     // passes once a half-warp lies inside one sub-row (TR >= 16).  Narrower sub-rows keep the
     // exchange layout's own stride rule.
     static constexpr int SB = TR >= 16 ? (smem_stride<B, E, false>() + 15) / 16 * 16 : smem_stride<B, E, false>();
-    static constexpr int NAT = spad(N - 1) + 1;           // natural-order staging extent
-    static constexpr int ROWBUF = (A * SB > NAT ? A * SB : NAT) | 1;
+    static constexpr int ROWBUF = A * SB | 1;
     static constexpr int CTA = T < 256 ? (256 / T) * T : T;
     static constexpr int ROWS = CTA / T;
     static constexpr int COLS = (B + T - 1) / T;          // columns of the A-point phase per thread
+    static constexpr int INV_B_MOD_A = mod_inverse(B % A, A);   // k1 = (k mod A) * B^-1 mod A
+    static constexpr int INV_A_MOD_B = mod_inverse(A % B, B);   // k2 =  k * A^-1 mod B
     // n <= 12288: the A = 15, n = 15360 variant would need 960 threads and spills its columns
     static_assert(A % 2 == 1 && B % E == 0 && N <= (int)backend::kPfaMaxN, "shape outside the instantiated family");
 };
@@ -153,7 +161,8 @@ k_pfa(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
         TB::for_each_out(v, t, [&](int k2, float2 x) { sub[spad(k2)] = x; });
     }
     __syncthreads();
-    // 3. A-point DFT down each column k2; outputs to X[(B k1 + A k2) mod n] in natural order
+    // 3. A-point DFT down each column k2; X[(B k1 + A k2) mod n] = Y[k1][k2] kept at
+    //    buf[k1*SB + k2] (unpadded: lanes hold consecutive k2, so the writes are contiguous)
     float2 w[A];
 #pragma unroll
     for (int m = 0; m < A; ++m) w[m] = __ldg(wA + m);
@@ -171,16 +180,19 @@ k_pfa(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
         if (k2 < B) {
             dft_odd<A, INV>(col[c], w);
 #pragma unroll
-            for (int k1 = 0; k1 < A; ++k1) buf[spad((B * k1 + A * k2) % N)] = col[c][k1];
+            for (int k1 = 0; k1 < A; ++k1) buf[k1 * P::SB + k2] = col[c][k1];
         }
     }
     __syncthreads();
-    // 4. coalesced stores
+    // 4. coalesced stores of X[k] = Y[k1][k2]; across lanes k2 steps by the odd A^-1 mod B,
+    //    a permutation of the banks
     if (ok) {
 #pragma unroll 4
         for (int i = 0; i < E; ++i) {
             const int k = tid + i * T;
-            st_stream(dst + k, cscale(buf[spad(k)], scale));
+            const int k1 = ((k % A) * P::INV_B_MOD_A) % A;
+            const int k2 = (k * P::INV_A_MOD_B) & (B - 1);
+            st_stream(dst + k, cscale(buf[k1 * P::SB + k2], scale));
         }
     }
 }
