@@ -33,6 +33,8 @@ int eventCreate(void** event);
 int eventDestroy(void* event);
 int eventRecord(void* event, void* stream);
 int streamWaitEvent(void* stream, void* event);   // later work on `stream` waits for `event`
+int eventSync(void* event);                       // host waits for `event`
+bool isPinnedHost(const void* ptr);               // page-locked (or registered) host memory
 
 // Device-side elapsed time between start() and stop() on one stream (CUDA events).
 struct Timer;

@@ -59,6 +59,15 @@ int eventCreate(void** event) {
 }
 int eventDestroy(void* event) { return rc(cudaEventDestroy(static_cast<cudaEvent_t>(event))); }
 int eventRecord(void* event, void* stream) { return rc(cudaEventRecord(static_cast<cudaEvent_t>(event), S(stream))); }
+int eventSync(void* event) { return rc(cudaEventSynchronize(static_cast<cudaEvent_t>(event))); }
+bool isPinnedHost(const void* ptr) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();   // an unknown pointer is ordinary pageable memory
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
 int streamWaitEvent(void* stream, void* event) {
     return rc(cudaStreamWaitEvent(S(stream), static_cast<cudaEvent_t>(event), 0));
 }

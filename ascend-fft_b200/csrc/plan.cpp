@@ -15,15 +15,22 @@
 #include "ragged.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <functional>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
 #include <sstream>
+#include <mutex>
 #include <stdexcept>
+#include <thread>
 #include <utility>
+#include <vector>
 
 namespace bfly {
 
@@ -352,6 +359,13 @@ struct Plan::Impl {
     void* ev[2] = {nullptr, nullptr};    // chunk uploaded / chunk transformed
     void* devHalf = nullptr;             // column-transformed half spectrum of execC2R2D
     size_t devHalfCap = 0;
+    // pinned staging for pageable host buffers: two slots per direction, with the events that
+    // say a slot's upload has read it / its download has filled it
+    void* pinIn[2] = {nullptr, nullptr};
+    void* pinOut[2] = {nullptr, nullptr};
+    size_t pinInCap = 0, pinOutCap = 0;
+    void* evStage[2] = {nullptr, nullptr};
+    void* evOut[2] = {nullptr, nullptr};
     void* tcTable[4] = {nullptr, nullptr, nullptr, nullptr};   // split DFT-16 operand per term count
     struct Chirp {
         void* chirp = nullptr;   // c[j] = exp(-i*pi*j^2/n), j < n
@@ -375,6 +389,12 @@ Plan::~Plan() {
     if (impl_->devOut) backend::release(impl_->devOut);
     if (impl_->devWork) backend::release(impl_->devWork);
     if (impl_->devHalf) backend::release(impl_->devHalf);
+    for (int i = 0; i < 2; ++i) {
+        if (impl_->pinIn[i]) backend::releaseHost(impl_->pinIn[i]);
+        if (impl_->pinOut[i]) backend::releaseHost(impl_->pinOut[i]);
+        if (impl_->evStage[i]) backend::eventDestroy(impl_->evStage[i]);
+        if (impl_->evOut[i]) backend::eventDestroy(impl_->evOut[i]);
+    }
     backend::timerDestroy(impl_->timer);
     for (void* st : impl_->aux)
         if (st) backend::streamDestroy(st);
@@ -768,6 +788,77 @@ static size_t chunkBytesFor(size_t bytes) {
     return std::min<size_t>(kChunkBytes, std::max<size_t>(2u << 20, bytes / 4));
 }
 
+namespace {
+// Process-wide host threads that split large copies between pageable and pinned memory (one
+// thread copies about 10 GB/s; the PCIe link wants 55 GB/s per direction).
+class CopyPool {
+public:
+    static CopyPool& get() {
+        static CopyPool pool;
+        return pool;
+    }
+    void copy(void* dst, const void* src, size_t bytes) {
+        const size_t parts = std::min<size_t>(workers_.size() + 1, std::max<size_t>(1, bytes >> 20));
+        if (parts <= 1) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        const size_t step = (bytes + parts - 1) / parts;
+        std::atomic<size_t> pending{parts - 1};
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            for (size_t p = 1; p < parts; ++p) {
+                const size_t off = std::min(bytes, p * step), len = std::min(step, bytes - off);
+                tasks_.push_back([=, &pending] {
+                    if (len) std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, len);
+                    if (--pending == 0) {
+                        std::lock_guard<std::mutex> done(doneMu_);
+                        doneCv_.notify_all();
+                    }
+                });
+            }
+        }
+        cv_.notify_all();
+        std::memcpy(dst, src, std::min(step, bytes));
+        std::unique_lock<std::mutex> lock(doneMu_);
+        doneCv_.wait(lock, [&] { return pending.load() == 0; });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+
+private:
+    CopyPool() {
+        const unsigned hc = std::thread::hardware_concurrency();
+        const unsigned n = hc > 2 ? std::min(hc / 2, 8u) - 1 : 0;
+        for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+    }
+    void loop() {
+        for (;;) {
+            std::function<void()> task;
+            {
+                std::unique_lock<std::mutex> lock(mu_);
+                cv_.wait(lock, [&] { return stop_ || !tasks_.empty(); });
+                if (stop_ && tasks_.empty()) return;
+                task = std::move(tasks_.front());
+                tasks_.pop_front();
+            }
+            task();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::deque<std::function<void()>> tasks_;
+    std::mutex mu_, doneMu_;
+    std::condition_variable cv_, doneCv_;
+    bool stop_ = false;
+};
+}  // namespace
+
 template <class Enqueue>
 int Plan::roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRowBytes,
                     uint32_t batch, Enqueue&& enqueue) {
@@ -799,6 +890,75 @@ int Plan::roundTrip(const float* in, size_t inRowBytes, float* out, size_t outRo
     void* sOut = im->aux[1];
     const size_t row = inRowBytes > outRowBytes ? inRowBytes : outRowBytes;
     const uint32_t chunk = (uint32_t)std::max<size_t>(1, chunkBytesFor(row * batch) / row);
+    if (!backend::isPinnedHost(in) || !backend::isPinnedHost(out)) {
+        // Pageable host buffers: the driver would stage them through its own small buffers
+        // (13 GB/s here).  Instead, host threads copy each chunk into one of two pinned slots
+        // while the GPU works on the previous chunk, and out of the result slot behind it.
+        const size_t inChunk = (size_t)chunk * inRowBytes, outChunk = (size_t)chunk * outRowBytes;
+        for (int i = 0; i < 2; ++i) {
+            if (im->pinInCap < inChunk && im->pinIn[i]) {
+                backend::releaseHost(im->pinIn[i]);
+                im->pinIn[i] = nullptr;
+            }
+            if (im->pinOutCap < outChunk && im->pinOut[i]) {
+                backend::releaseHost(im->pinOut[i]);
+                im->pinOut[i] = nullptr;
+            }
+        }
+        for (int i = 0; i < 2; ++i) {
+            if (!im->pinIn[i] && backend::allocHost(&im->pinIn[i], std::max(inChunk, im->pinInCap))) {
+                im->pinIn[i] = nullptr;
+                return -3;
+            }
+            if (!im->pinOut[i] && backend::allocHost(&im->pinOut[i], std::max(outChunk, im->pinOutCap))) {
+                im->pinOut[i] = nullptr;
+                return -3;
+            }
+            if (!im->evStage[i] && backend::eventCreate(&im->evStage[i])) im->evStage[i] = nullptr;
+            if (!im->evOut[i] && backend::eventCreate(&im->evOut[i])) im->evOut[i] = nullptr;
+            if (!im->evStage[i] || !im->evOut[i]) return -3;
+        }
+        im->pinInCap = std::max(im->pinInCap, inChunk);
+        im->pinOutCap = std::max(im->pinOutCap, outChunk);
+        auto drain = [&](int code) {   // nothing may still read or fill a slot after an error
+            backend::streamSync(sIn);
+            backend::streamSync(stream_);
+            backend::streamSync(sOut);
+            return code;
+        };
+        CopyPool& pool = CopyPool::get();
+        const uint32_t chunks = (batch + chunk - 1) / chunk;
+        auto finishOut = [&](uint32_t k) -> int {
+            const uint32_t r0 = k * chunk, rows = std::min(chunk, batch - r0);
+            if (backend::eventSync(im->evOut[k & 1])) return -7;
+            pool.copy(reinterpret_cast<char*>(out) + (size_t)r0 * outRowBytes, im->pinOut[k & 1],
+                      (size_t)rows * outRowBytes);
+            return 0;
+        };
+        for (uint32_t k = 0; k < chunks; ++k) {
+            const uint32_t r0 = k * chunk, rows = std::min(chunk, batch - r0);
+            const int s = (int)(k & 1);
+            if (k >= 2 && backend::eventSync(im->evStage[s])) return drain(-4);   // slot s read by chunk k-2
+            pool.copy(im->pinIn[s], reinterpret_cast<const char*>(in) + (size_t)r0 * inRowBytes,
+                      (size_t)rows * inRowBytes);
+            char* di = static_cast<char*>(im->devIn) + (size_t)r0 * inRowBytes;
+            char* dout = static_cast<char*>(im->devOut) + (size_t)r0 * outRowBytes;
+            if (backend::copyH2D(di, im->pinIn[s], (size_t)rows * inRowBytes, sIn)) return drain(-4);
+            if (backend::eventRecord(im->evStage[s], sIn) || backend::streamWaitEvent(stream_, im->evStage[s]))
+                return drain(-6);
+            const int lrc = enqueue(di, dout, r0, rows, stream_);
+            if (lrc == -2 || lrc == -3) return drain(lrc);
+            if (lrc) return drain(-5);
+            if (backend::eventRecord(im->ev[1], stream_) || backend::streamWaitEvent(sOut, im->ev[1])) return drain(-6);
+            if (backend::copyD2H(im->pinOut[s], dout, (size_t)rows * outRowBytes, sOut)) return drain(-7);
+            if (backend::eventRecord(im->evOut[s], sOut)) return drain(-6);
+            if (k >= 1)
+                if (int rc = finishOut(k - 1)) return drain(rc);
+        }
+        if (int rc = finishOut(chunks - 1)) return drain(rc);
+        if (backend::streamSync(sIn) || backend::streamSync(stream_)) return -6;
+        return backend::streamSync(sOut) ? -6 : 0;
+    }
     for (uint32_t r0 = 0; r0 < batch; r0 += chunk) {
         const uint32_t rows = std::min(chunk, batch - r0);
         char* di = static_cast<char*>(im->devIn) + (size_t)r0 * inRowBytes;

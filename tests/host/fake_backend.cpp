@@ -16,6 +16,7 @@ int allocations = 0, releases = 0, copies = 0, launches = 0, syncs = 0;
 int failAllocation = 0, failCopy = 0, failLaunch = 0, failSync = 0;   // 1-based call index
 int streamsCreated = 0, streamsDestroyed = 0;
 int deviceCountValue = 1;
+bool pageableHost = false;   // report host buffers as pageable (staged round trips)
 float timerMs = 0.01f;   // reported time per launch
 }  // namespace fake
 
@@ -65,6 +66,8 @@ int eventCreate(void** e) { *e = reinterpret_cast<void*>(0x2); return 0; }
 int eventDestroy(void*) { return 0; }
 int eventRecord(void*, void*) { return 0; }
 int streamWaitEvent(void*, void*) { return 0; }
+int eventSync(void*) { return 0; }
+bool isPinnedHost(const void*) { return !fake::pageableHost; }
 int alloc(void** p, size_t bytes) {
     ++fake::allocations;
     if (fake::allocations == fake::failAllocation) { *p = nullptr; return 2; }

@@ -23,6 +23,7 @@ extern int allocations, releases, copies, launches, syncs;
 extern int failAllocation, failCopy, failLaunch, failSync;
 extern int streamsCreated, streamsDestroyed, deviceCountValue;
 extern float timerMs;
+extern bool pageableHost;
 }  // namespace fake
 
 #define CHECK(cond)                                                                    \
@@ -516,6 +517,22 @@ int main(int argc, char** argv) {
         const bfly::HostRequest bad4[] = {reqs[0], {a.data(), oa.data(), 64, 0, -1, 1.f}};
         for (const auto* bad : {bad1, bad2, bad3, bad4}) CHECK(plan->runMany(bad, 2) == -8);
         CHECK(fake::allocations == allocBefore && fake::copies == copiesBefore && fake::launches == launchBefore);
+    }
+
+    {   // pageable host buffers go through pinned staging slots: same results as the direct path
+        const uint32_t n = 64, batch = 20000;   // 10 MB each way: five pipeline chunks
+        std::vector<float> x(2 * (size_t)n * batch), yDirect(x.size()), yStaged(x.size());
+        for (size_t i = 0; i < x.size(); ++i) x[i] = (float)std::sin(0.001 * i + (i % 5));
+        CHECK(plan->run(x.data(), yDirect.data(), n, batch) == 0);
+        fake::pageableHost = true;
+        CHECK(plan->run(x.data(), yStaged.data(), n, batch) == 0);
+        CHECK(yStaged == yDirect);
+        fake::failCopy = fake::copies + 3;          // a later upload fails
+        CHECK(plan->run(x.data(), yStaged.data(), n, batch) == -4);
+        fake::failCopy = 0;
+        CHECK(plan->run(x.data(), yStaged.data(), n, batch) == 0);   // the plan stays usable
+        CHECK(yStaged == yDirect);
+        fake::pageableHost = false;
     }
 
     plan.reset();

@@ -48,3 +48,35 @@ def test_run_many_guards(plan):
     assert plan.run_many([]) == -8
     assert plan.run_many([(x, y, 64, 2), (x, y, 9000, 1)]) == -8
     assert plan.run_many([(x, y, 64, 2, 0, 1.0)]) == -8
+
+
+@pytest.mark.parametrize("kind", ["c2c", "r2c", "c2r"])
+def test_pageable_round_trip_matches_exec(plan, cuda, kind):
+    """Large transfers from ordinary (pageable) host memory go through the plan's pinned staging
+    slots; results must equal the device entry point's bit for bit."""
+    import torch
+    n, batch = (4096, 3000) if kind == "c2c" else (2048, 6000)
+    rng = np.random.default_rng(3)
+    if kind == "c2c":
+        x = rng.standard_normal((batch, 2 * n)).astype(np.float32)
+        y = np.empty_like(x)
+        assert plan.run(x, y, n, batch) == 0
+        xd = torch.from_numpy(x).to(cuda)
+        yd = torch.empty_like(xd)
+        assert plan.exec_c2c(xd.data_ptr(), yd.data_ptr(), n, batch, -1, 1.0, 0) == 0
+    elif kind == "r2c":
+        x = rng.standard_normal((batch, n)).astype(np.float32)
+        y = np.empty((batch, n + 2), np.float32)
+        assert plan.run_r2c(x, y, n, batch) == 0
+        xd = torch.from_numpy(x).to(cuda)
+        yd = torch.empty(batch, n + 2, device=cuda)
+        assert plan.exec_r2c(xd.data_ptr(), yd.data_ptr(), n, batch, 1.0, 1.0, 0) == 0
+    else:
+        x = rng.standard_normal((batch, n + 2)).astype(np.float32)
+        y = np.empty((batch, n), np.float32)
+        assert plan.run_c2r(x, y, n, batch) == 0
+        xd = torch.from_numpy(x).to(cuda)
+        yd = torch.empty(batch, n, device=cuda)
+        assert plan.exec_c2r(xd.data_ptr(), yd.data_ptr(), n, batch, 1.0, 1.0, 1.0 / n, 0) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(y, yd.cpu().numpy())
