@@ -142,11 +142,16 @@ k_pfa(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     float2* dst = out + row * N;
     float2* buf = smem + rl * P::ROWBUF;
 
-    // 1. coalesced loads, scattered to [j mod A][j mod B]
+    // 1. coalesced loads, scattered to [j mod A][j mod B].  T is a multiple of A, so
+    //    j mod A = tid mod A for every j = tid + i*T this thread loads.
+    static_assert(T % A == 0, "the n-row team size is a multiple of A");
+    {
+        float2* rowA = buf + (tid % A) * P::SB;
 #pragma unroll 4
-    for (int i = 0; i < E; ++i) {
-        const int j = tid + i * T;
-        buf[(j % A) * P::SB + spad(j % B)] = ok ? ld_stream(src + j) : make_float2(0.f, 0.f);
+        for (int i = 0; i < E; ++i) {
+            const int j = tid + i * T;
+            rowA[spad(j & (B - 1))] = ok ? ld_stream(src + j) : make_float2(0.f, 0.f);
+        }
     }
     __syncthreads();
     // 2. B-point FFT of sub-row j1 by sub-team j1, results back in natural order k2
@@ -187,12 +192,14 @@ k_pfa(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     // 4. coalesced stores of X[k] = Y[k1][k2]; across lanes k2 steps by the odd A^-1 mod B,
     //    a permutation of the banks
     if (ok) {
+        // k mod A = tid mod A for all k = tid + i*T, so k1 is fixed; k2 steps by T*A^-1 mod B
+        const float2* rowK = buf + (((tid % A) * P::INV_B_MOD_A) % A) * P::SB;
+        constexpr int STEP = (int)(((long long)T * P::INV_A_MOD_B) & (B - 1));
+        int k2 = (tid * P::INV_A_MOD_B) & (B - 1);
 #pragma unroll 4
         for (int i = 0; i < E; ++i) {
-            const int k = tid + i * T;
-            const int k1 = ((k % A) * P::INV_B_MOD_A) % A;
-            const int k2 = (k * P::INV_A_MOD_B) & (B - 1);
-            st_stream(dst + k, cscale(buf[k1 * P::SB + k2], scale));
+            st_stream(dst + tid + i * T, cscale(rowK[k2], scale));
+            k2 = (k2 + STEP) & (B - 1);
         }
     }
 }
