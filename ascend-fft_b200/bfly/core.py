@@ -190,6 +190,14 @@ class Plan:
                                                  stream or None)
         return rc, frames.value
 
+    def exec_istft(self, d_spec: int, d_out: int, n: int, signals: int, frames: int, hop: int,
+                   center: bool = True, d_window: int = 0, out_len: int = 0, scale: float = 1.0,
+                   stream: int = 0) -> int:
+        """Inverse STFT of [signals][frames][n/2+1] complex64 into [signals][out_len] float32."""
+        return self._lib.bfly_plan_exec_istft_async(self._h, d_spec, d_out, n, signals, frames, hop,
+                                                    1 if center else 0, d_window or None, out_len, scale,
+                                                    stream or None)
+
     def exec_r2c(self, d_in: int, d_out: int, n: int, batch: int, s_edge: float = 1.0,
                  s_int: float = 1.0, stream: int = 0) -> int:
         return self._lib.bfly_plan_exec_r2c_async(self._h, d_in, d_out, n, batch, s_edge, s_int,

@@ -11,6 +11,8 @@ hand-written adjoints behind torch.autograd.Function:
     stft(x, n_fft, ...)     float32 [..., L] -> complex64 [..., n_fft/2+1, frames], torch.stft's
                             arguments and defaults (centred reflect padding, hop n_fft/4); framing,
                             window and one-sided transform in one kernel
+    istft(X, n_fft, ...)    complex64 [..., n_fft/2+1, frames] -> float32 [..., L], torch.istft's
+                            arguments; C2R of every frame, then a windowed overlap-add kernel
     rfft(x)                 float32 [..., n] -> complex64 [..., n/2+1], n in 64..8192
     irfft(X, n)             complex64 [..., n/2+1] -> float32 [..., n]
 
@@ -340,26 +342,138 @@ class _STFT(torch.autograd.Function):
         return gx, None, None, None, None
 
 
-def stft(x: torch.Tensor, n_fft: int, hop_length: int | None = None, window: torch.Tensor | None = None,
-         center: bool = True, pad_mode: str = "reflect", normalized: bool = False,
-         onesided: bool = True, return_complex: bool = True) -> torch.Tensor:
-    """torch.stft on the fused kernel: float32 [..., L] -> complex64 [..., n_fft/2+1, frames]."""
+def stft(x: torch.Tensor, n_fft: int, hop_length: int | None = None, win_length: int | None = None,
+         window: torch.Tensor | None = None, center: bool = True, pad_mode: str = "reflect",
+         normalized: bool = False, onesided: bool | None = None,
+         return_complex: bool | None = None) -> torch.Tensor:
+    """torch.stft on the fused kernel: float32 [..., L] -> complex64 [..., n_fft/2+1, frames].
+    Arguments in torch.stft's order and with its defaults (a window shorter than n_fft is
+    centred with zeros)."""
     _need_cuda(x, torch.float32, "stft")
-    if not return_complex or not onesided:
+    if return_complex is False or onesided is False:
         raise ValueError("stft: only onesided=True, return_complex=True are supported")
     if center and pad_mode != "reflect":
         raise ValueError("stft: only pad_mode='reflect' is supported")
     hop = hop_length if hop_length is not None else n_fft // 4
-    if window is not None:
-        _need_cuda(window, torch.float32, "stft window")
-        if window.shape != (n_fft,):
-            raise ValueError(f"stft: window must have shape ({n_fft},)")
-        window = window.contiguous()
+    window = _pad_window(window, win_length, n_fft, "stft window", x.device)
     if normalized:
         window = (window if window is not None else torch.ones(n_fft, device=x.device)) * n_fft ** -0.5
     lead = x.shape[:-1]
     y = _STFT.apply(x.contiguous().reshape(-1, x.shape[-1]), n_fft, hop, center, window)
     return y.reshape(*lead, y.shape[-2], y.shape[-1]).transpose(-1, -2)
+
+
+class _ISTFT(torch.autograd.Function):
+    """Inverse transform of every frame + windowed overlap-add divided by the squared-window
+    envelope.  Adjoint: h = g / envelope on the padded timeline (zero outside the kept samples),
+    then the uncentred windowed STFT of h, weighted like irfft's adjoint (bins 0 and n/2 by c,
+    the others by 2c, c = scale / n)."""
+
+    @staticmethod
+    def forward(ctx, spec, n, hop, center, window, out_len, scale):
+        signals, frames = spec.shape[0], spec.shape[1]
+        y = torch.empty(signals, out_len, dtype=torch.float32, device=spec.device)
+        rc = plan_for(spec.device, n, "real").exec_istft(
+            spec.data_ptr(), y.data_ptr(), n, signals, frames, hop, center,
+            window.data_ptr() if window is not None else 0, out_len, scale, _stream(spec))
+        if rc:
+            raise BflyError(f"exec_istft(n={n}, signals={signals}, frames={frames}, hop={hop})", rc)
+        ctx.n, ctx.hop, ctx.center, ctx.scale, ctx.frames = n, hop, center, scale, frames
+        ctx.save_for_backward(window)
+        return y
+
+    @staticmethod
+    def backward(ctx, g):
+        (window,) = ctx.saved_tensors
+        n, hop, frames = ctx.n, ctx.hop, ctx.frames
+        padded = n + hop * (frames - 1)
+        start = n // 2 if ctx.center else 0
+        env = _envelope(window, n, hop, frames, g.device)
+        keep = max(0, min(g.shape[1], padded - start))
+        h = torch.zeros(g.shape[0], padded, dtype=torch.float32, device=g.device)
+        e = env[start:start + keep]
+        h[:, start:start + keep] = torch.where(e > 0, g[:, :keep] / torch.where(e > 0, e, 1.0), 0.0)
+        gs = torch.empty(g.shape[0], frames, n // 2 + 1, dtype=torch.complex64, device=g.device)
+        rc, got = plan_for(g.device, n, "real").exec_stft(
+            h.data_ptr(), gs.data_ptr(), n, g.shape[0], padded, hop, False,
+            window.data_ptr() if window is not None else 0, _stream(g))
+        if rc or got != frames:
+            raise BflyError(f"exec_stft (istft adjoint, n={n}, frames={frames})", rc or -1)
+        c = ctx.scale / n
+        wt = torch.full((n // 2 + 1,), 2.0 * c, dtype=torch.float32, device=g.device)
+        wt[0] = wt[-1] = c
+        return gs * wt, None, None, None, None, None, None
+
+
+def _envelope(window, n: int, hop: int, frames: int, device) -> torch.Tensor:
+    """Overlap-added squared window over the padded timeline, n + hop*(frames-1) samples."""
+    w2 = (window * window) if window is not None else torch.ones(n, device=device)
+    cols = w2.reshape(1, n, 1).expand(1, n, frames)
+    padded = n + hop * (frames - 1)
+    return torch.nn.functional.fold(cols, output_size=(1, padded), kernel_size=(1, n),
+                                    stride=(1, hop)).reshape(padded)
+
+
+_envelope_checked = {}   # (window ptr, version, n, hop, frames, start, length) already verified
+
+
+def _pad_window(window, win_length, n_fft, what, device):
+    """torch.stft / torch.istft window handling: shape (win_length,), centred in n_fft with zeros."""
+    if window is None:
+        if win_length is None or win_length == n_fft:
+            return None
+        window = torch.ones(win_length, dtype=torch.float32, device=device)
+    _need_cuda(window, torch.float32, what)
+    wl = win_length if win_length is not None else n_fft
+    if window.shape != (wl,) or wl > n_fft or wl < 1:
+        raise ValueError(f"{what}: window must have shape ({wl},) with win_length <= n_fft")
+    if wl < n_fft:
+        left = (n_fft - wl) // 2
+        window = torch.nn.functional.pad(window, (left, n_fft - wl - left))
+    return window.contiguous()
+
+
+def istft(X: torch.Tensor, n_fft: int, hop_length: int | None = None, win_length: int | None = None,
+          window: torch.Tensor | None = None, center: bool = True, normalized: bool = False,
+          onesided: bool | None = None, length: int | None = None,
+          return_complex: bool = False) -> torch.Tensor:
+    """torch.istft on the device kernels: complex64 [..., n_fft/2+1, frames] -> float32 [..., L].
+
+    Every frame is inverse-transformed (irfft, 1/n_fft), multiplied by the window and overlap-
+    added; each sample is divided by the overlap-added squared window, as torch.istft does, and
+    a window envelope below 1e-11 inside the kept samples raises like torch.istft."""
+    _need_cuda(X, torch.complex64, "istft")
+    if return_complex or onesided is False:
+        raise ValueError("istft: only onesided input and real output are supported")
+    if X.dim() < 2 or X.shape[-2] != n_fft // 2 + 1:
+        raise ValueError(f"istft: expected [..., {n_fft // 2 + 1}, frames], got {tuple(X.shape)}")
+    hop = hop_length if hop_length is not None else n_fft // 4
+    if hop <= 0 or hop > n_fft:
+        raise ValueError(f"istft: hop_length must be in [1, n_fft], got {hop}")
+    window = _pad_window(window, win_length, n_fft, "istft window", X.device)
+    frames = X.shape[-1]
+    padded = n_fft + hop * (frames - 1)
+    start = n_fft // 2 if center else 0
+    out_len = length if length is not None else padded - 2 * start
+    if out_len <= 0:
+        raise ValueError("istft: empty output")
+    # the envelope of the kept samples must not vanish (torch.istft's check); verified once per
+    # window contents and geometry
+    key = (window.data_ptr() if window is not None else 0, window._version if window is not None else 0,
+           X.device.index, n_fft, hop, frames, start, out_len)
+    if key not in _envelope_checked:
+        env = _envelope(window, n_fft, hop, frames, X.device)[start:start + out_len]
+        if env.numel() and float(env.min()) < 1e-11:
+            raise RuntimeError("istft: window overlap-add envelope is zero inside the output "
+                               "(the window and hop do not satisfy the NOLA condition)")
+        if len(_envelope_checked) > 256:
+            _envelope_checked.clear()
+        _envelope_checked[key] = True
+    lead = X.shape[:-2]
+    spec = X.reshape(-1, X.shape[-2], frames).transpose(-1, -2).contiguous()
+    scale = n_fft ** 0.5 if normalized else 1.0
+    y = _ISTFT.apply(spec, n_fft, hop, center, window, out_len, scale)
+    return y.reshape(*lead, out_len)
 
 
 class _RFFT2(torch.autograd.Function):

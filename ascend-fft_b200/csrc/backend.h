@@ -113,6 +113,11 @@ int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_
                uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,
                const void* tw, const void* twr, void* stream);
 
+// Overlap-add (inverse STFT): out[s][i] = sum_f w[j] fr[s][f][j] / sum_f w[j]^2 over the frames
+// covering padded position i + start (j = i + start - f*hop); fr = [signals][frames][n] floats.
+int launchOla(const void* frames, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal, uint32_t hop,
+              int64_t start, uint64_t outLen, const void* window, void* stream);
+
 // Column FFTs: ny-point transforms down the ncols columns of `mats` row-major matrices,
 // element (m, i, col) at m*matStride + i*pitch + col (float2 units).  ny in 32..4096;
 // tw = Stockham table (ny, 16); in == out allowed.

@@ -208,6 +208,13 @@ int bfly_plan_exec_stft_async(bfly_plan* plan, const void* d_sig, void* d_out, u
     return p.execStft(d_sig, d_out, n, signals, sig_len, hop, center != 0, d_window, frames, stream);
 }
 
+int bfly_plan_exec_istft_async(bfly_plan* plan, const void* d_spec, void* d_out, uint32_t n,
+                               uint64_t signals, uint32_t frames, uint32_t hop, int center,
+                               const void* d_window, uint64_t out_len, float scale, void* stream) {
+    PLAN_OR_FAIL();
+    return p.execIstft(d_spec, d_out, n, signals, frames, hop, center != 0, d_window, out_len, scale, stream);
+}
+
 int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, float s_edge, float s_int, void* stream) {
     PLAN_OR_FAIL();

@@ -77,6 +77,33 @@ k_stft(const float* __restrict__ sig, float2* __restrict__ out, const float2* __
     if (t == 0) bin(M, wm);
 }
 
+// Overlap-add of inverse-transformed frames (the second half of an inverse STFT), gather form:
+//   out[s][i] = sum_f w[j] fr[s][f][j] / sum_f w[j]^2,   j = i + start - f*hop, 0 <= j < n,
+// with w = 1 when window is null; start = n/2 removes the centring pad.  One thread per output
+// sample; the frames covering it are read at consecutive j by consecutive threads.  Samples
+// whose envelope is zero are written as 0 (the caller checks the envelope beforehand).
+static __global__ void k_ola(const float* __restrict__ fr, float* __restrict__ out, const float* __restrict__ window,
+                             uint32_t n, uint32_t frames, uint32_t hop, int64_t start, uint64_t outLen,
+                             uint64_t signals) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= outLen * signals) return;
+    const uint64_t s = g / outLen, i = g % outLen;
+    const int64_t p = (int64_t)i + start;   // position in the padded signal
+    const float* f0 = fr + s * (uint64_t)frames * n;
+    int64_t fhi = p / hop;
+    if (fhi > (int64_t)frames - 1) fhi = (int64_t)frames - 1;
+    int64_t flo = p - (int64_t)n + 1 > 0 ? (p - (int64_t)n + hop) / hop : 0;
+    float acc = 0.f, env = 0.f;
+    for (int64_t f = flo; f <= fhi; ++f) {
+        const int64_t j = p - f * (int64_t)hop;
+        if (j < 0 || j >= (int64_t)n) continue;
+        const float w = window ? __ldg(window + j) : 1.f;
+        acc += w * __ldg(f0 + (uint64_t)f * n + j);
+        env += w * w;
+    }
+    out[g] = env > 0.f ? acc / env : 0.f;
+}
+
 }  // namespace dev
 
 namespace backend {
@@ -104,6 +131,18 @@ int launchStftN(const float* sig, void* out, uint64_t rows, uint32_t framesPerSi
 }  // namespace
 
 bool hasStft(uint32_t n) { return n >= kStftMinN && n <= kStftMaxN && !(n & (n - 1)); }
+
+int launchOla(const void* frames, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal, uint32_t hop,
+              int64_t start, uint64_t outLen, const void* window, void* stream) {
+    const uint64_t total = outLen * signals;
+    if (total == 0) return 0;
+    const uint64_t blocks = (total + 255) / 256;
+    if (blocks > 0x7fffffffull) return (int)cudaErrorInvalidValue;
+    dev::k_ola<<<(unsigned)blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<const float*>(frames), static_cast<float*>(out), static_cast<const float*>(window), n,
+        framesPerSignal, hop, start, outLen, signals);
+    return (int)cudaGetLastError();
+}
 
 int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal,
                uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,

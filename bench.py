@@ -423,10 +423,19 @@ def extra_measurements(dev, stream):
         ref = torch.stft(x[:1, :16 * n].double(), n, hop_length=hop, window=w.double(), return_complex=True)[..., :8]
         got = y[:1, :8].transpose(-1, -2).to(torch.complex128)
         err = float((torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)).item())
+        # inverse STFT of the same spectrum back to the 4 signals; bytes = spectrum read + signal
+        # written (the two-kernel path also writes and reads every frame once in between)
+        xb = torch.empty(S, L, device=dev)
+        ms_i = timed(lambda: plan.exec_istft(y.data_ptr(), xb.data_ptr(), n, S, frames, hop, True, w.data_ptr(), L,
+                                             1.0, sh))
+        ib = S * frames * 8 * (n // 2 + 1) + 4 * S * L
+        rt = float((torch.linalg.vector_norm(xb - x) / torch.linalg.vector_norm(x)).item())
         out["stft"][f"n{n}_hop{hop}_S{S}_L{L}"] = {"frame_gbs": round(fb / ms / 1e6, 1),
                                                     "frac": round(fb / ms / 1e6 / peak, 4), "rel_l2": err,
-                                                    "frames": S * frames}
-        del x, y
+                                                    "frames": S * frames,
+                                                    "istft_gbs": round(ib / ms_i / 1e6, 1),
+                                                    "istft_ms": round(ms_i, 4), "round_trip_rel_l2": rt}
+        del x, y, xb
     # ---- real transforms: R2C forward and its adjoint (weighted C2R), batch 1024
     for n in (128, 1024, 4096, 8192):
         b = 1024

@@ -122,9 +122,24 @@ int launchR2C(const void*, void*, uint32_t, uint64_t, const void*, const void*, 
               float, float, void*) {
     return launch();
 }
-int launchC2R(const void*, void*, uint32_t, uint64_t, const void*, const void*, int, int, float,
-              float, float, void*) {
-    return launch();
+// Direct inverse real DFT (numpy.fft.irfft semantics: imaginary parts of bins 0 and n/2 ignored).
+int launchC2R(const void* in, void* out, uint32_t n, uint64_t batch, const void*, const void*, int, int,
+              float sEdge, float sInt, float outScale, void*) {
+    if (int r = launch()) return r;
+    const uint32_t m = n / 2;
+    for (uint64_t b = 0; b < batch; ++b) {
+        const float* X = (const float*)in + b * 2 * (m + 1);
+        float* x = (float*)out + b * n;
+        for (uint32_t j = 0; j < n; ++j) {
+            double acc = sEdge * (X[0] + ((j & 1) ? -X[2 * m] : X[2 * m]));
+            for (uint32_t k = 1; k < m; ++k) {
+                const double a = 2 * M_PI * (double)(((uint64_t)j * k) % n) / n;
+                acc += 2.0 * sInt * (X[2 * k] * std::cos(a) - X[2 * k + 1] * std::sin(a));
+            }
+            x[j] = (float)(acc * outScale);
+        }
+    }
+    return 0;
 }
 
 bool hasLongSplit(uint32_t n1, uint32_t n2) { return n1 >= 32 && n1 <= 256 && n2 == 256; }
@@ -205,6 +220,27 @@ int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_
             dft(frame.data(), spec.data(), n, -1, 1.f);
             float* o = (float*)out + 2 * ((s * framesPerSignal + f) * (n / 2 + 1));
             std::memcpy(o, spec.data(), (n / 2 + 1) * 8);
+        }
+    return 0;
+}
+
+int launchOla(const void* frames, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal, uint32_t hop,
+              int64_t start, uint64_t outLen, const void* window, void*) {
+    if (int r = launch()) return r;
+    const float* fr = (const float*)frames;
+    const float* w = (const float*)window;
+    for (uint64_t s = 0; s < signals; ++s)
+        for (uint64_t i = 0; i < outLen; ++i) {
+            const long long p = (long long)i + start;
+            double acc = 0, env = 0;
+            for (uint32_t f = 0; f < framesPerSignal; ++f) {
+                const long long j = p - (long long)f * hop;
+                if (j < 0 || j >= (long long)n) continue;
+                const double wj = w ? w[j] : 1.0;
+                acc += wj * fr[(s * framesPerSignal + f) * n + j];
+                env += wj * wj;
+            }
+            ((float*)out)[s * outLen + i] = env > 0 ? (float)(acc / env) : 0.f;
         }
     return 0;
 }

@@ -494,6 +494,49 @@ int main(int argc, char** argv) {
         CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
     }
 
+    {   // inverse STFT: STFT then ISTFT gives the signal back (Hann window, centred, hop n/4),
+        // one C2R and one overlap-add launch, frame buffer allocated once; guards first
+        const uint32_t n = 64, hop = 16;
+        const uint64_t len = 256, signals = 2, frames = 1 + len / hop;
+        std::vector<float> sig(len * signals), win(n), back(len * signals, -1.f);
+        std::vector<float> spec(2 * (n / 2 + 1) * frames * signals);
+        for (size_t i = 0; i < sig.size(); ++i) sig[i] = (float)std::sin(0.11 * i + std::cos(0.03 * i));
+        for (uint32_t j = 0; j < n; ++j) win[j] = (float)(0.5 - 0.5 * std::cos(2 * M_PI * j / n));
+        float* d = sig.data();
+        const int allocBefore = fake::allocations, launchBefore = fake::launches;
+        CHECK(plan->execIstft(nullptr, d, n, 1, frames, hop, true, nullptr, len, 1.f, nullptr) == -8);
+        CHECK(plan->execIstft(d, d, 96, 1, frames, hop, true, nullptr, len, 1.f, nullptr) == -8);   // not a power of two
+        CHECK(plan->execIstft(d, d, n, 1, frames, 0, true, nullptr, len, 1.f, nullptr) == -8);     // hop 0
+        CHECK(plan->execIstft(d, d, n, 1, frames, n + 1, true, nullptr, len, 1.f, nullptr) == -8); // hop above n
+        CHECK(plan->execIstft(d, d, n, 0, frames, hop, true, nullptr, len, 1.f, nullptr) == -8);   // no signals
+        CHECK(plan->execIstft(d, d, n, 1, 0, hop, true, nullptr, len, 1.f, nullptr) == -8);        // no frames
+        CHECK(plan->execIstft(d, d, n, 1, frames, hop, true, nullptr, 0, 1.f, nullptr) == -8);     // empty output
+        CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
+        uint64_t got = 0;
+        CHECK(plan->execStft(sig.data(), spec.data(), n, signals, len, hop, true, win.data(), &got, nullptr) == 0);
+        CHECK(got == frames);
+        for (int rep = 0; rep < 2; ++rep) {
+            const int a0 = fake::allocations, l0 = fake::launches;
+            CHECK(plan->execIstft(spec.data(), back.data(), n, signals, (uint32_t)frames, hop, true, win.data(), len,
+                                  1.f, nullptr) == 0);
+            CHECK(fake::launches == l0 + 2);
+            CHECK(fake::allocations == a0 + (rep == 0 ? 1 : 0));
+        }
+        double e = 0;
+        for (size_t i = 0; i < sig.size(); ++i) e = std::max(e, (double)std::fabs(back[i] - sig[i]));
+        CHECK(e < 1e-4);
+        // uncentred, rectangular window, scale 2: frames cover [0, n + (frames-1) hop) exactly
+        const uint64_t fr2 = 1 + (len - n) / hop, out2 = n + (fr2 - 1) * hop;
+        CHECK(plan->execStft(sig.data(), spec.data(), n, 1, len, hop, false, nullptr, &got, nullptr) == 0);
+        CHECK(got == fr2);
+        CHECK(plan->execIstft(spec.data(), back.data(), n, 1, (uint32_t)fr2, hop, false, nullptr, out2 + 5, 2.f,
+                              nullptr) == 0);
+        e = 0;
+        for (uint64_t i = 0; i < out2; ++i) e = std::max(e, (double)std::fabs(back[i] - 2 * sig[i]));
+        for (uint64_t i = out2; i < out2 + 5; ++i) e = std::max(e, (double)std::fabs(back[i]));   // past the frames: 0
+        CHECK(e < 1e-4);
+    }
+
     {   // batched host round trip: equal to per-request device transforms; guards first
         std::vector<float> a(2 * 64 * 3), b(2 * 96 * 2), c(2 * 128 * 4);
         for (size_t i = 0; i < a.size(); ++i) a[i] = (float)std::sin(0.3 * i);
