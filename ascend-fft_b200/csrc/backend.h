@@ -113,10 +113,16 @@ int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_
                uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,
                const void* tw, const void* twr, void* stream);
 
-// Overlap-add (inverse STFT): out[s][i] = sum_f w[j] fr[s][f][j] / sum_f w[j]^2 over the frames
-// covering padded position i + start (j = i + start - f*hop); fr = [signals][frames][n] floats.
-int launchOla(const void* frames, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal, uint32_t hop,
-              int64_t start, uint64_t outLen, const void* window, void* stream);
+// Inverse STFT in one kernel: out[s][i] = y[i + start], y[p] = sum_f w[j] x_f[j] / sum_f w[j]^2
+// (j = p - f*hop in [0, n), x_f = scale/n * irfft of spec[s][f], window null = 1), zero past the
+// last frame; spec = [signals][frames][n/2+1] float2, hop <= n, tables as for launchStft.
+// Work split: signal s, segment c of q frames per CTA, `rows` frames per wave; istftSegments
+// picks q for `slots` resident CTAs on the device.
+void istftSegments(uint32_t n, int rows, uint32_t frames, uint32_t hop, uint64_t signals, uint64_t slots,
+                   uint32_t* q, uint32_t* segs);
+int launchIstft(const void* spec, void* out, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
+                int64_t start, uint64_t outLen, const void* window, const void* tw, const void* twr, float scale,
+                void* stream);
 
 // Column FFTs: ny-point transforms down the ncols columns of `mats` row-major matrices,
 // element (m, i, col) at m*matStride + i*pitch + col (float2 units).  ny in 32..4096;

@@ -106,6 +106,21 @@ k_r2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
 //   Xk = X[k], Xm = X[M-k] (scaled by s_edge at DC/Nyquist, s_int elsewhere),
 //   Z[k] = (Xk + conj Xm) + i (Xk - conj Xm) W_N^-k,  z = IDFT_M(Z) * out_scale,
 //   x[2m] = Re z[m], x[2m+1] = Im z[m].   out_scale = 1/N gives numpy.fft.irfft.
+// C2R split of bin k: xk = X[k], xm = X[M-k] (xm = X[M] for k = 0), twk = W_N^k.
+__device__ __forceinline__ float2 c2r_split(float2 xk, float2 xm, int k, float2 twk, float s_edge, float s_int,
+                                            float out_scale) {
+    if (k == 0) {
+        xk = make_float2(xk.x * s_edge, 0.f);
+        xm = make_float2(xm.x * s_edge, 0.f);
+    } else {
+        xk = cscale(xk, s_int);
+        xm = cscale(xm, s_int);
+    }
+    const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
+    const float2 od = cmul<true>(make_float2(xk.x - xm.x, xk.y + xm.y), twk);
+    return make_float2((ev.x - od.y) * out_scale, (ev.y + od.x) * out_scale);
+}
+
 template <int N, int E, int ROWS>
 __global__ void __launch_bounds__((N / 2 / E) * ROWS, min_blocks_64regs((N / 2 / E) * ROWS))
 k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
@@ -132,18 +147,7 @@ k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     for (int i = 0; i < E; ++i) sm[spad(t + i * T)] = v[i];
     TM::sync(rl);
     TM::load_first(v, t, [&](int k) {
-        float2 xk = sm[spad(k)];
-        float2 xm = k == 0 ? nyq : sm[spad(M - k)];
-        if (k == 0) {
-            xk = make_float2(xk.x * s_edge, 0.f);
-            xm = make_float2(xm.x * s_edge, 0.f);
-        } else {
-            xk = cscale(xk, s_int);
-            xm = cscale(xm, s_int);
-        }
-        const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
-        const float2 od = cmul<true>(make_float2(xk.x - xm.x, xk.y + xm.y), __ldg(twr + k));
-        return make_float2((ev.x - od.y) * out_scale, (ev.y + od.x) * out_scale);
+        return c2r_split(sm[spad(k)], k == 0 ? nyq : sm[spad(M - k)], k, __ldg(twr + k), s_edge, s_int, out_scale);
     });
     TM::sync(rl);   // the passes reuse the staging buffer for their exchanges
     TM::template passes<0>(v, sm, tw, t, rl);

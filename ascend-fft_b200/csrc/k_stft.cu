@@ -77,31 +77,191 @@ k_stft(const float* __restrict__ sig, float2* __restrict__ out, const float2* __
     if (t == 0) bin(M, wm);
 }
 
-// Overlap-add of inverse-transformed frames (the second half of an inverse STFT), gather form:
-//   out[s][i] = sum_f w[j] fr[s][f][j] / sum_f w[j]^2,   j = i + start - f*hop, 0 <= j < n,
-// with w = 1 when window is null; start = n/2 removes the centring pad.  One thread per output
-// sample; the frames covering it are read at consecutive j by consecutive threads.  Samples
-// whose envelope is zero are written as 0 (the caller checks the envelope beforehand).
-static __global__ void k_ola(const float* __restrict__ fr, float* __restrict__ out, const float* __restrict__ window,
-                             uint32_t n, uint32_t frames, uint32_t hop, int64_t start, uint64_t outLen,
-                             uint64_t signals) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= outLen * signals) return;
-    const uint64_t s = g / outLen, i = g % outLen;
-    const int64_t p = (int64_t)i + start;   // position in the padded signal
-    const float* f0 = fr + s * (uint64_t)frames * n;
-    int64_t fhi = p / hop;
-    if (fhi > (int64_t)frames - 1) fhi = (int64_t)frames - 1;
-    int64_t flo = p - (int64_t)n + 1 > 0 ? (p - (int64_t)n + hop) / hop : 0;
-    float acc = 0.f, env = 0.f;
-    for (int64_t f = flo; f <= fhi; ++f) {
-        const int64_t j = p - f * (int64_t)hop;
-        if (j < 0 || j >= (int64_t)n) continue;
-        const float w = window ? __ldg(window + j) : 1.f;
-        acc += w * __ldg(f0 + (uint64_t)f * n + j);
-        env += w * w;
+// Inverse STFT in one kernel (torch.istft): every frame's C2R, window, overlap-add and the
+// division by the overlap-added squared window, each output sample written once.
+//   y[p] = sum_f w[j] x_f[j] / sum_f w[j]^2,  j = p - f*hop in [0, N),  x_f = out_scale * IDFT_N
+//   (spec[s][f]) with the imaginary parts of bins 0 and N/2 ignored;  out[s][i] = y[i + start],
+//   i < outLen, zero past the last frame.
+// CTA (s, c) owns padded samples [c*Q*hop, (c+1)*Q*hop) of signal s (the last CTA of a signal
+// also the tail).  It transforms frames c*Q - (K-1) .. (c+1)*Q - 1 (K = ceil(N/hop) frames cover
+// a sample) in waves of ROWS frames: each frame's C2R runs in registers, the windowed result
+// lands in the row's shared buffer, then all threads sum, per sample of the wave's span, the
+// carried partial sum of earlier frames and the wave's frames covering it.  Samples no later
+// frame touches are complete and stored, times 1 / envelope (a per-CTA table over p mod hop,
+// exact sums within a frame of either end); the rest (N - hop samples) are carried to the next
+// wave in the other half of a ping-pong buffer.  Frames before the CTA's first sample only fill
+// the carry, so K - 1 frames per CTA are transformed twice (Q is chosen so that costs < 7%).
+// Summation order is fixed (frames in increasing order), so results are deterministic.
+// Row stride of the inverse-STFT row buffers: the team's exchange stride rounded up to even.
+template <int M, int E>
+__host__ __device__ constexpr int istft_row_stride() {
+    return smem_stride<M, E, false>() + (smem_stride<M, E, false>() & 1);
+}
+
+template <int N, int E, int ROWS, int MINB, int VEC>
+__global__ void __launch_bounds__((N / 2 / E) * ROWS, MINB)
+k_istft(const float2* __restrict__ spec, float* __restrict__ out, const float2* __restrict__ tw,
+        const float2* __restrict__ twr, const float* __restrict__ window, uint32_t frames, uint32_t hop, uint32_t Q,
+        uint32_t segs, int64_t start, uint64_t outLen, float out_scale) {
+    constexpr int M = N / 2;
+    constexpr int T = M / E;
+    constexpr int CTA = T * ROWS;
+    constexpr int S = istft_row_stride<M, E>();   // even: every row buffer 16-byte aligned
+    static_assert(2 * S >= N, "a row buffer holds one real frame");
+    static_assert(VEC == 1 || VEC == 4, "scalar or float4 overlap-add");
+    using TM = Team<M, E, true, sync_kind(T, CTA)>;
+    extern __shared__ float2 smem[];
+    const int rl = threadIdx.x / T;
+    const int t = threadIdx.x - rl * T;
+    const uint32_t s = blockIdx.x / segs;
+    const uint32_t c = blockIdx.x - s * segs;
+    const int K = (N + (int)hop - 1) / (int)hop;
+    const int CARRY = N - (int)hop;
+    const int64_t padded = (int64_t)N + (int64_t)hop * (frames - 1);
+    const uint64_t first = (uint64_t)c * Q;
+    const uint32_t fA = first >= (uint64_t)(K - 1) ? (uint32_t)(first - (K - 1)) : 0u;
+    const uint32_t fB = (uint32_t)min((uint64_t)frames, first + Q);
+    const int64_t P0 = (int64_t)first * hop;
+    const int64_t end = start + (int64_t)outLen;
+    const int64_t P1 = c + 1 == segs ? (padded > end ? padded : end) : (int64_t)fB * hop;
+    const float2* src0 = spec + (uint64_t)s * frames * (M + 1);
+    float* dst = out + (uint64_t)s * outLen;
+    float2* sm = smem + rl * S;
+    float* cur = reinterpret_cast<float*>(smem + ROWS * S);
+    float* nxt = cur + CARRY;
+    // 1 / (overlap-added squared window) of samples every frame slot of which exists
+    // (N-1 <= p < frames*hop): periodic in p with period hop
+    float* rinv = nxt + CARRY;
+    for (int q = threadIdx.x; q < CARRY; q += CTA) cur[q] = 0.f;
+    for (int r = threadIdx.x; r < (int)hop; r += CTA) {
+        float e = 0.f;
+        for (int j = r; j < N; j += (int)hop) {
+            const float w = window ? __ldg(window + j) : 1.f;
+            e += w * w;
+        }
+        rinv[r] = e > 0.f ? 1.f / e : 0.f;
     }
-    out[g] = env > 0.f ? acc / env : 0.f;
+    // samples near either end: the envelope of the frames that exist
+    auto edgeInv = [&](int64_t p) {
+        float e = 0.f;
+        const int64_t fh = p / hop;
+        for (int64_t f = fh - K + 1 > 0 ? fh - K + 1 : 0; f <= fh && f < (int64_t)frames; ++f) {
+            const int64_t j = p - f * hop;
+            if (j < N) {
+                const float w = window ? __ldg(window + j) : 1.f;
+                e += w * w;
+            }
+        }
+        return e > 0.f ? 1.f / e : 0.f;
+    };
+    // each thread sums VEC consecutive samples: q += VEC*CTA, tracked as (q / hop, q % hop)
+    const int stepH = VEC * CTA / (int)hop, stepR = VEC * CTA - stepH * (int)hop;
+    const int qh0 = VEC * (int)threadIdx.x / (int)hop, qr0 = VEC * (int)threadIdx.x - qh0 * (int)hop;
+    auto clampq = [](int64_t v, int hi) { return (int)(v < 0 ? 0 : (v > hi ? hi : v)); };
+
+    for (uint32_t f0 = fA; f0 < fB; f0 += ROWS) {
+        const int R = (int)min((uint32_t)ROWS, fB - f0);
+        // rows past R (a CTA's partial first or last wave) transform frame f0 again and are not
+        // read: every row runs the same barriers, rows of one warp included
+        const float2* src = src0 + (uint64_t)(f0 + (rl < R ? rl : 0)) * (M + 1);
+        const float2 nyq = t == 0 ? ld_stream(src + M) : make_float2(0.f, 0.f);
+        float2 v[E];
+#pragma unroll
+        for (int i = 0; i < E; ++i) v[i] = ld_stream(src + t + i * T);
+        __syncthreads();   // the previous wave is done with the row buffers and the carry
+#pragma unroll
+        for (int i = 0; i < E; ++i) sm[spad(t + i * T)] = v[i];
+        TM::sync(rl);
+        TM::load_first(v, t, [&](int k) {
+            return c2r_split(sm[spad(k)], k == 0 ? nyq : sm[spad(M - k)], k, __ldg(twr + k), 1.f, 1.f, out_scale);
+        });
+        TM::sync(rl);
+        TM::template passes<0>(v, sm, tw, t, rl);
+        TM::sync(rl);
+        TM::for_each_out(v, t, [&](int i, float2 z) {   // windowed frame: samples 2i, 2i+1 at sm[i]
+            const float2 w = window ? __ldg(reinterpret_cast<const float2*>(window) + i) : make_float2(1.f, 1.f);
+            sm[i] = make_float2(z.x * w.x, z.y * w.y);
+        });
+        __syncthreads();
+        const bool tail = f0 + R == frames;   // no later frame: every sample of the span is complete
+        const int span = (R - 1) * (int)hop + N;
+        const int done = tail ? span : R * (int)hop;
+        const int64_t base = (int64_t)f0 * hop;
+        // span offsets q this CTA stores ([wlo, whi)) and those with the periodic envelope
+        const int wlo = clampq((P0 > start ? P0 : start) - base, done);
+        const int whi = clampq((P1 < end ? P1 : end) - base, done);
+        const int elo = clampq((int64_t)(N - 1) - base, span);
+        const int ehi = clampq((int64_t)frames * hop - base, span);
+        float* dq = dst + (base - start);   // output of span offset q at dq[q] (wlo <= q < whi)
+        int qh = qh0, qr = qr0;
+        if constexpr (VEC == 1) {
+            for (int q = threadIdx.x; q < span; q += CTA) {
+                float val = q < CARRY ? cur[q] : 0.f;
+                const int rlo = qh - K + 1 > 0 ? qh - K + 1 : 0;
+                const int rhi = qh < R - 1 ? qh : R - 1;
+                for (int r = rlo; r <= rhi; ++r) {
+                    const int j = qr + (qh - r) * (int)hop;
+                    if (j < N) val += reinterpret_cast<const float*>(smem + r * S)[j];
+                }
+                if (q >= done) {
+                    nxt[q - done] = val;
+                } else if (q >= wlo && q < whi) {
+                    __stcs(dq + q, val * (q >= elo && q < ehi ? rinv[qr] : edgeInv(base + q)));
+                }
+                qh += stepH;
+                qr += stepR;
+                if (qr >= (int)hop) {
+                    qr -= (int)hop;
+                    ++qh;
+                }
+            }
+        } else {
+            // hop, N, CARRY, done, wlo and whi are multiples of 4 and the 4 samples share q / hop:
+            // every shared and global access below is one aligned float4
+            for (int q = 4 * threadIdx.x; q < span; q += 4 * CTA) {
+                float4 val = q < CARRY ? *reinterpret_cast<const float4*>(cur + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const int rlo = qh - K + 1 > 0 ? qh - K + 1 : 0;
+                const int rhi = qh < R - 1 ? qh : R - 1;
+                for (int r = rlo; r <= rhi; ++r) {
+                    const int j = qr + (qh - r) * (int)hop;
+                    if (j < N) {
+                        const float4 x = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(smem + r * S) + j);
+                        val.x += x.x;
+                        val.y += x.y;
+                        val.z += x.z;
+                        val.w += x.w;
+                    }
+                }
+                if (q >= done) {
+                    *reinterpret_cast<float4*>(nxt + q - done) = val;
+                } else if (q >= wlo && q < whi) {
+                    float4 e;
+                    if (q >= elo && q + 3 < ehi) {
+                        e = *reinterpret_cast<const float4*>(rinv + qr);
+                    } else {
+                        auto inv = [&](int u) { return q + u >= elo && q + u < ehi ? rinv[qr + u] : edgeInv(base + q + u); };
+                        e = make_float4(inv(0), inv(1), inv(2), inv(3));
+                    }
+                    __stcs(reinterpret_cast<float4*>(dq + q), make_float4(val.x * e.x, val.y * e.y, val.z * e.z, val.w * e.w));
+                }
+                qh += stepH;
+                qr += stepR;
+                if (qr >= (int)hop) {
+                    qr -= (int)hop;
+                    ++qh;
+                }
+            }
+        }
+        float* sw = cur;
+        cur = nxt;
+        nxt = sw;
+    }
+    if (c + 1 == segs) {   // samples past the last frame up to outLen are zero
+        for (int64_t p = (padded > P0 ? padded : P0) + threadIdx.x; p < P1; p += CTA) {
+            const int64_t i = p - start;
+            if (i >= 0 && i < (int64_t)outLen) __stcs(dst + i, 0.f);
+        }
+    }
 }
 
 }  // namespace dev
@@ -128,21 +288,63 @@ int launchStftN(const float* sig, void* out, uint64_t rows, uint32_t framesPerSi
     return (int)cudaGetLastError();
 }
 
-}  // namespace
-
-bool hasStft(uint32_t n) { return n >= kStftMinN && n <= kStftMaxN && !(n & (n - 1)); }
-
-int launchOla(const void* frames, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal, uint32_t hop,
-              int64_t start, uint64_t outLen, const void* window, void* stream) {
-    const uint64_t total = outLen * signals;
-    if (total == 0) return 0;
-    const uint64_t blocks = (total + 255) / 256;
-    if (blocks > 0x7fffffffull) return (int)cudaErrorInvalidValue;
-    dev::k_ola<<<(unsigned)blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        static_cast<const float*>(frames), static_cast<float*>(out), static_cast<const float*>(window), n,
-        framesPerSignal, hop, start, outLen, signals);
+template <int N>
+int launchIstftN(const float2* spec, float* out, uint64_t signals, uint32_t frames, uint32_t hop, int64_t start,
+                 uint64_t outLen, const float* window, const void* tw, const void* twr, float scale, void* stream) {
+    constexpr int M = N / 2, E = 16, T = M / E;
+    constexpr int CTA = T < 256 ? 256 : T;
+    constexpr int ROWS = CTA / T;
+    constexpr int ROWBYTES = ROWS * dev::istft_row_stride<M, E>() * 8;
+    // N >= 2048: shared memory holds at most 3 CTAs per SM, so up to 80 registers a thread
+    constexpr int MINB = N >= 2048 ? 3 : dev::min_blocks_64regs(CTA);
+    // float4 overlap-add when the frame starts and the output rows keep 16-byte alignment
+    const bool vec = hop % 4 == 0 && outLen % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
+    auto* fn = vec ? dev::k_istft<N, E, ROWS, MINB, 4> : dev::k_istft<N, E, ROWS, MINB, 1>;
+    if (int e = optInSharedMemory((const void*)fn, ROWBYTES + 3 * N * 4)) return e;
+    const int smem = ROWBYTES + (2 * (N - (int)hop) + (int)hop) * 4;
+    int device = 0, sms = 0, perSm = 0;
+    if (cudaGetDevice(&device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, CTA, smem) != cudaSuccess || perSm < 1)
+        return (int)cudaErrorInvalidConfiguration;
+    uint32_t q, segs;
+    istftSegments(N, ROWS, frames, hop, signals, (uint64_t)sms * perSm, &q, &segs);
+    const uint64_t grid = signals * segs;
+    if (grid > 0x7fffffffull) return (int)cudaErrorInvalidValue;
+    fn<<<(unsigned)grid, CTA, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        spec, out, static_cast<const float2*>(tw), static_cast<const float2*>(twr), window, frames, hop, q, segs,
+        start, outLen, scale / N);
     return (int)cudaGetLastError();
 }
+
+}  // namespace
+
+void istftSegments(uint32_t n, int rows, uint32_t frames, uint32_t hop, uint64_t signals, uint64_t slots,
+                   uint32_t* q, uint32_t* segs) {
+    // A CTA transforms m*rows frames (m waves), K-1 of them warm-up frames, and stores
+    // Q = m*rows - (K-1) frames' worth of samples.  Estimated time = rounds of resident CTAs x
+    // waves per CTA; the smallest wins, ties going to the larger m (fewer warm-up frames).
+    const uint32_t k1 = (n + hop - 1) / hop - 1;
+    const uint64_t r = (uint64_t)rows;
+    const uint64_t mlo = (k1 + 1 + r - 1) / r;
+    const uint64_t mhi = (17ull * k1 + (k1 ? 0 : 16) + r - 1) / r + 64;
+    uint64_t best = ~0ull;
+    *q = (uint32_t)(mlo * r - k1);
+    *segs = (uint32_t)((frames + *q - 1) / *q);
+    for (uint64_t m = mlo; m <= mhi; ++m) {
+        const uint64_t qq = m * r - k1;
+        const uint64_t sg = (frames + qq - 1) / qq;
+        const uint64_t rounds = (signals * sg + slots - 1) / (slots ? slots : 1);
+        if (rounds * m <= best) {
+            best = rounds * m;
+            *q = (uint32_t)qq;
+            *segs = (uint32_t)sg;
+        }
+        if (sg == 1) break;
+    }
+}
+
+bool hasStft(uint32_t n) { return n >= kStftMinN && n <= kStftMaxN && !(n & (n - 1)); }
 
 int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal,
                uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,
@@ -164,6 +366,29 @@ int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_
         default: return (int)cudaErrorInvalidValue;
     }
 #undef BFLY_ST
+}
+
+int launchIstft(const void* spec, void* out, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
+                int64_t start, uint64_t outLen, const void* window, const void* tw, const void* twr, float scale,
+                void* stream) {
+    if (!hasStft(n) || hop == 0 || hop > n || frames == 0) return (int)cudaErrorInvalidValue;
+    const float2* x = static_cast<const float2*>(spec);
+    float* y = static_cast<float*>(out);
+    const float* w = static_cast<const float*>(window);
+#define BFLY_IS(N) \
+    case N: return launchIstftN<N>(x, y, signals, frames, hop, start, outLen, w, tw, twr, scale, stream)
+    switch (n) {
+        BFLY_IS(64);
+        BFLY_IS(128);
+        BFLY_IS(256);
+        BFLY_IS(512);
+        BFLY_IS(1024);
+        BFLY_IS(2048);
+        BFLY_IS(4096);
+        BFLY_IS(8192);
+        default: return (int)cudaErrorInvalidValue;
+    }
+#undef BFLY_IS
 }
 
 }  // namespace backend

@@ -359,8 +359,6 @@ struct Plan::Impl {
     void* ev[2] = {nullptr, nullptr};    // chunk uploaded / chunk transformed
     void* devHalf = nullptr;             // column-transformed half spectrum of execC2R2D
     size_t devHalfCap = 0;
-    void* devFrames = nullptr;           // inverse-transformed frames of execIstft
-    size_t devFramesCap = 0;
     // pinned staging for pageable host buffers: two slots per direction, with the events that
     // say a slot's upload has read it / its download has filled it
     void* pinIn[2] = {nullptr, nullptr};
@@ -391,7 +389,6 @@ Plan::~Plan() {
     if (impl_->devOut) backend::release(impl_->devOut);
     if (impl_->devWork) backend::release(impl_->devWork);
     if (impl_->devHalf) backend::release(impl_->devHalf);
-    if (impl_->devFrames) backend::release(impl_->devFrames);
     for (int i = 0; i < 2; ++i) {
         if (impl_->pinIn[i]) backend::releaseHost(impl_->pinIn[i]);
         if (impl_->pinOut[i]) backend::releaseHost(impl_->pinOut[i]);
@@ -736,12 +733,10 @@ int Plan::execIstft(const void* dSpec, void* dOut, uint32_t n, uint64_t signals,
                     bool center, const void* dWindow, uint64_t outLen, float scale, void* stream) {
     if (!impl_ || !dSpec || !dOut || signals == 0 || frames == 0 || hop == 0 || hop > n || !backend::hasStft(n))
         return -8;
-    if (signals * frames > 0xFFFFFFFFull || outLen == 0) return -8;
-    // inverse transform of every frame (numpy.fft.irfft) into a plan-owned frame buffer
-    if (ensureBuf(&impl_->devFrames, &impl_->devFramesCap, (size_t)signals * frames * n * 4)) return -3;
-    if (int r = execC2R(dSpec, impl_->devFrames, n, signals * frames, 1.0f, 1.0f, scale / n, stream)) return r;
-    if (backend::launchOla(impl_->devFrames, dOut, n, signals, frames, hop, center ? (int64_t)(n / 2) : 0, outLen,
-                           dWindow, stream))
+    if (signals * frames > 0xFFFFFFFFull || outLen == 0 || outLen > (1ull << 62)) return -8;
+    if (prepareC2C(n / 2, kColsE) || prepareReal(n)) return -2;
+    if (backend::launchIstft(dSpec, dOut, n, signals, frames, hop, center ? (int64_t)(n / 2) : 0, outLen, dWindow,
+                             impl_->twC2C[{n / 2, kColsE}], impl_->twReal[n], scale, stream))
         return -5;
     return 0;
 }

@@ -678,7 +678,7 @@ def run_case(spec: str, reps: int):
     spec = kind:n:batch with kind in c2c, c2c_inv (any n: non-powers of two run the Bluestein
     kernel), tc2, tc3 (tensor-core splits), r2c, c2r, cluster (long C2C on the cluster
     schedule), or ragged:grid:CAP; or cols:NY:NCOLS:MATS (column kernel), c2d:NY:NX:B (2-D),
-    stft:N:HOP:LEN (4 signals, centred, Hann window)."""
+    stft:N:HOP:LEN (4 signals, centred, Hann window), istft:N:HOP:LEN (its inverse)."""
     import torch
     import bfly
     parts = spec.split(":")
@@ -687,7 +687,7 @@ def run_case(spec: str, reps: int):
     ctx = bfly.Context()
     assert ctx.init() == 0
     plan = ctx.make_plan()
-    if kind in ("cols", "c2d", "stft"):
+    if kind in ("cols", "c2d", "stft", "istft"):
         a, b2, c = (int(v) for v in parts[1:4])
         g = torch.Generator(device=dev).manual_seed(a + b2 + c)
         if kind == "cols":     # NY-point transforms down NCOLS columns of MATS matrices
@@ -698,11 +698,17 @@ def run_case(spec: str, reps: int):
             x = torch.randn(c, a, b2, dtype=torch.complex64, device=dev, generator=g)
             y = torch.empty_like(x)
             call = lambda: plan.exec_c2c_2d(x.data_ptr(), y.data_ptr(), a, b2, c, -1, 1.0, 0)
-        else:                  # stft:N:HOP:LEN
+        elif kind == "stft":   # stft:N:HOP:LEN
             x = torch.randn(4, c, device=dev, generator=g)
             w = torch.hann_window(a, device=dev)
             y = torch.empty(4, 1 + c // b2, a // 2 + 1, dtype=torch.complex64, device=dev)
             call = lambda: plan.exec_stft(x.data_ptr(), y.data_ptr(), a, 4, c, b2, True, w.data_ptr())[0]
+        else:                  # istft:N:HOP:LEN
+            fr = 1 + c // b2
+            x = torch.randn(4, fr, a // 2 + 1, dtype=torch.complex64, device=dev, generator=g)
+            w = torch.hann_window(a, device=dev)
+            y = torch.empty(4, c, device=dev)
+            call = lambda: plan.exec_istft(x.data_ptr(), y.data_ptr(), a, 4, fr, b2, True, w.data_ptr(), c, 1.0, 0)
         for _ in range(reps):
             r = call()
             if r:

@@ -123,9 +123,8 @@ int launchR2C(const void*, void*, uint32_t, uint64_t, const void*, const void*, 
     return launch();
 }
 // Direct inverse real DFT (numpy.fft.irfft semantics: imaginary parts of bins 0 and n/2 ignored).
-int launchC2R(const void* in, void* out, uint32_t n, uint64_t batch, const void*, const void*, int, int,
-              float sEdge, float sInt, float outScale, void*) {
-    if (int r = launch()) return r;
+static void c2rDirect(const void* in, void* out, uint32_t n, uint64_t batch, float sEdge, float sInt,
+                      float outScale) {
     const uint32_t m = n / 2;
     for (uint64_t b = 0; b < batch; ++b) {
         const float* X = (const float*)in + b * 2 * (m + 1);
@@ -139,6 +138,12 @@ int launchC2R(const void* in, void* out, uint32_t n, uint64_t batch, const void*
             x[j] = (float)(acc * outScale);
         }
     }
+}
+
+int launchC2R(const void* in, void* out, uint32_t n, uint64_t batch, const void*, const void*, int, int,
+              float sEdge, float sInt, float outScale, void*) {
+    if (int r = launch()) return r;
+    c2rDirect(in, out, n, batch, sEdge, sInt, outScale);
     return 0;
 }
 
@@ -224,24 +229,35 @@ int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_
     return 0;
 }
 
-int launchOla(const void* frames, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal, uint32_t hop,
-              int64_t start, uint64_t outLen, const void* window, void*) {
+void istftSegments(uint32_t n, int rows, uint32_t frames, uint32_t hop, uint64_t signals, uint64_t slots,
+                   uint32_t* q, uint32_t* segs) {
+    *q = frames;
+    *segs = 1;
+    (void)n, (void)rows, (void)hop, (void)signals, (void)slots;
+}
+
+// C2R of every frame (scale/n), windowed overlap-add, division by the squared-window envelope.
+int launchIstft(const void* spec, void* out, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
+                int64_t start, uint64_t outLen, const void* window, const void*, const void*, float scale, void*) {
+    if (!hasStft(n) || hop == 0 || hop > n || frames == 0) return 1;
     if (int r = launch()) return r;
-    const float* fr = (const float*)frames;
     const float* w = (const float*)window;
-    for (uint64_t s = 0; s < signals; ++s)
+    std::vector<float> fr((size_t)frames * n);
+    for (uint64_t s = 0; s < signals; ++s) {
+        c2rDirect((const float*)spec + s * frames * (n + 2), fr.data(), n, frames, 1.f, 1.f, scale / n);
         for (uint64_t i = 0; i < outLen; ++i) {
             const long long p = (long long)i + start;
             double acc = 0, env = 0;
-            for (uint32_t f = 0; f < framesPerSignal; ++f) {
+            for (uint32_t f = 0; f < frames; ++f) {
                 const long long j = p - (long long)f * hop;
                 if (j < 0 || j >= (long long)n) continue;
                 const double wj = w ? w[j] : 1.0;
-                acc += wj * fr[(s * framesPerSignal + f) * n + j];
+                acc += wj * fr[(size_t)f * n + j];
                 env += wj * wj;
             }
             ((float*)out)[s * outLen + i] = env > 0 ? (float)(acc / env) : 0.f;
         }
+    }
     return 0;
 }
 
