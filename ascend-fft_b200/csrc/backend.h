@@ -103,6 +103,41 @@ int buildBluesteinTables(void* chirp, void* filt, void* scratch, uint32_t n, voi
 int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
                     const void* tw, const void* chirp, const void* filt, void* stream);
 
+// Mixed-radix C2C for 7-smooth lengths n = 2^a 3^b 5^c 7^d in [2, kMixedMaxN]: Stockham passes
+// of radix 16, 8, 4, 2, 7, 5, 3 (in that order) through shared memory, one kernel; tw = W_n^m,
+// m < n (linear table of n entries).  mixedRadix fills the pass list (false when n is not
+// 7-smooth or out of range); ns[p] = product of the radices before pass p.
+constexpr uint32_t kMixedMaxN = 12288;
+constexpr int kMixedMaxPasses = 16;
+struct MixedRadix {
+    int n = 0, passes = 0;
+    int radix[kMixedMaxPasses] = {};
+    int ns[kMixedMaxPasses] = {};
+};
+inline bool mixedRadix(uint32_t n, MixedRadix* m) {
+    if (n < 2 || n > kMixedMaxN) return false;
+    uint32_t rest = n;
+    MixedRadix r;
+    r.n = (int)n;
+    auto push = [&](int radix) {
+        r.ns[r.passes] = r.passes ? r.ns[r.passes - 1] * r.radix[r.passes - 1] : 1;
+        r.radix[r.passes++] = radix;
+        rest /= (uint32_t)radix;
+    };
+    while (rest % 16 == 0) push(16);
+    if (rest % 8 == 0) push(8);
+    if (rest % 4 == 0) push(4);
+    if (rest % 2 == 0) push(2);
+    static constexpr int kOdd[3] = {7, 5, 3};
+    for (int p : kOdd)
+        while (rest % (uint32_t)p == 0) push(p);
+    if (rest != 1) return false;
+    if (m) *m = r;
+    return true;
+}
+int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
+                const void* tw, void* stream);
+
 // STFT: `signals` real signals of sigLen samples (signal s at s*sigStride floats), frames of n
 // samples every `hop` (centred with reflect padding when `center`), times `window` (n floats,
 // or null for none), R2C of each frame into out[s][f][n/2+1].  n a power of two in

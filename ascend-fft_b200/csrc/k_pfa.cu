@@ -12,44 +12,10 @@
 
 #include "backend.h"
 #include "fft_kernels.cuh"
+#include "fft_odd.cuh"
 
 namespace bfly {
 namespace dev {
-
-// ------------------------------------------------------------------ small odd DFTs
-// Forward sign exp(-2*pi*i/A); INV flips it.  Constants are cos/sin of 2*pi/3, 2*pi/5, 4*pi/5.
-__device__ __forceinline__ float2 mul_i(float2 a, bool neg) {   // -i*a (neg) or +i*a
-    return neg ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
-}
-
-template <bool INV>
-__device__ __forceinline__ void dft3(float2& x0, float2& x1, float2& x2) {
-    constexpr float kS3 = 0.866025403784438647f;   // sin(2*pi/3)
-    const float2 t1 = cadd(x1, x2);
-    const float2 t2 = make_float2(x1.x - x2.x, x1.y - x2.y);
-    const float2 m = make_float2(x0.x - 0.5f * t1.x, x0.y - 0.5f * t1.y);
-    const float2 r = mul_i(make_float2(kS3 * t2.x, kS3 * t2.y), !INV);
-    x0 = cadd(x0, t1);
-    x1 = cadd(m, r);
-    x2 = make_float2(m.x - r.x, m.y - r.y);
-}
-
-template <bool INV>
-__device__ __forceinline__ void dft5(float2& x0, float2& x1, float2& x2, float2& x3, float2& x4) {
-    constexpr float kC1 = 0.309016994374947424f, kC2 = -0.809016994374947424f;   // cos(2pi/5), cos(4pi/5)
-    constexpr float kS1 = 0.951056516295153572f, kS2 = 0.587785252292473129f;    // sin(2pi/5), sin(4pi/5)
-    const float2 t1 = cadd(x1, x4), t2 = cadd(x2, x3);
-    const float2 t3 = make_float2(x1.x - x4.x, x1.y - x4.y), t4 = make_float2(x2.x - x3.x, x2.y - x3.y);
-    const float2 a1 = make_float2(x0.x + kC1 * t1.x + kC2 * t2.x, x0.y + kC1 * t1.y + kC2 * t2.y);
-    const float2 a2 = make_float2(x0.x + kC2 * t1.x + kC1 * t2.x, x0.y + kC2 * t1.y + kC1 * t2.y);
-    const float2 b1 = mul_i(make_float2(kS1 * t3.x + kS2 * t4.x, kS1 * t3.y + kS2 * t4.y), !INV);
-    const float2 b2 = mul_i(make_float2(kS2 * t3.x - kS1 * t4.x, kS2 * t3.y - kS1 * t4.y), !INV);
-    x0 = cadd(x0, cadd(t1, t2));
-    x1 = cadd(a1, b1);
-    x4 = make_float2(a1.x - b1.x, a1.y - b1.y);
-    x2 = cadd(a2, b2);
-    x3 = make_float2(a2.x - b2.x, a2.y - b2.y);
-}
 
 // In-place A-point DFT of x (natural order in and out); w = W_A^m, m < A (used by A = 9).
 template <int A, bool INV>

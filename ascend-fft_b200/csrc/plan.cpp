@@ -373,6 +373,7 @@ struct Plan::Impl {
     };
     std::map<uint32_t, Chirp> bluestein;   // non-power-of-two n -> Bluestein tables
     std::map<uint32_t, void*> dftSmall;    // A -> W_A^m, m < A (prime-factor kernels)
+    std::map<uint32_t, void*> mixedTw;     // 7-smooth n -> W_n^m, m < n (mixed-radix kernel)
 };
 
 Plan::Plan(Candidate c) : cand_(std::move(c)) {}
@@ -404,6 +405,8 @@ Plan::~Plan() {
         if (t) backend::release(t);
     for (auto& kv : impl_->dftSmall)
         if (kv.second) backend::release(kv.second);
+    for (auto& kv : impl_->mixedTw)
+        if (kv.second) backend::release(kv.second);
     for (auto& kv : impl_->bluestein) {
         if (kv.second.chirp) backend::release(kv.second.chirp);
         if (kv.second.filt) backend::release(kv.second.filt);
@@ -428,10 +431,12 @@ static int ensureBuf(void** p, size_t* cap, size_t bytes) {
 bool Plan::validShape(uint32_t n, uint32_t batch, int kind) const {
     if (!impl_ || batch == 0) return false;
     // lengths outside the power-of-two kernels (non-powers of two, and 2..16) only through the
-    // device-pointer C2C entry (prime-factor kernel for A*2^k, else Bluestein)
+    // device-pointer C2C entry (prime-factor kernel for A*2^k, mixed radix for other 7-smooth
+    // lengths, else Bluestein)
     if (!pow2(n) || (kind == kExecC2C && n < kMinN)) {
         uint32_t a = 0, b = 0;
-        return kind == kExecC2C && (backend::bluesteinM(n) != 0 || backend::pfaSplit(n, &a, &b));
+        return kind == kExecC2C &&
+               (backend::bluesteinM(n) != 0 || backend::pfaSplit(n, &a, &b) || backend::mixedRadix(n, nullptr));
     }
     const bool offsetGuard = kind == kRunC2C || kind == kRunR2C || kind == kRunC2R ||
                              kind == kRunLong || kind == kMeasure;
@@ -555,6 +560,26 @@ int Plan::preparePfa(uint32_t n) {
     return 0;
 }
 
+int Plan::prepareMixed(uint32_t n) {
+    if (!backend::mixedRadix(n, nullptr)) return -1;
+    if (impl_->mixedTw.count(n)) return 0;
+    void* w = nullptr;
+    if (backend::alloc(&w, (size_t)n * 8)) return -1;
+    if (backend::buildLinearTwiddles(w, (int)n, 1, n, stream_) || backend::streamSync(stream_)) {
+        backend::release(w);
+        return -1;
+    }
+    impl_->mixedTw[n] = w;
+    return 0;
+}
+
+int Plan::prepareAnyLength(uint32_t n) {
+    uint32_t a = 0, b = 0;
+    if (!pow2(n) && backend::pfaSplit(n, &a, &b)) return preparePfa(n);
+    if (backend::mixedRadix(n, nullptr)) return prepareMixed(n);
+    return prepareBluestein(n);
+}
+
 int Plan::prepareBluestein(uint32_t n) {
     const uint32_t M = backend::bluesteinM(n);
     if (!M || prepareC2C(M, kColsE)) return -1;
@@ -611,6 +636,12 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
         if (preparePfa(n)) return -2;
         if (backend::launchPfa(dIn, dOut, n, batch, inv, scale, impl_->twC2C[{pb, kColsE}], impl_->dftSmall[pa], s))
             return -5;
+        return 0;
+    }
+    backend::MixedRadix mr;
+    if ((!pow2(n) || n < kMinN) && backend::mixedRadix(n, &mr)) {   // other 7-smooth lengths
+        if (prepareMixed(n)) return -2;
+        if (backend::launchMixed(dIn, dOut, mr, batch, inv, scale, impl_->mixedTw[n], s)) return -5;
         return 0;
     }
     if (!pow2(n) || n < kMinN) {   // Bluestein: one kernel on the padded power-of-two length
@@ -1013,7 +1044,7 @@ int Plan::runMany(const HostRequest* reqs, size_t count) {
                 const size_t rows = std::min<size_t>(r.batch, std::max<size_t>(1, kChunkBytes / ((size_t)r.n * 8)));
                 workElems = std::max(workElems, rows * r.n);
             }
-        } else if (prepareBluestein(r.n)) {
+        } else if (prepareAnyLength(r.n)) {
             return -2;
         }
     }

@@ -275,6 +275,8 @@ private:
     int prepareLong(uint32_t n);
     int prepareBluestein(uint32_t n);
     int preparePfa(uint32_t n);
+    int prepareMixed(uint32_t n);
+    int prepareAnyLength(uint32_t n);   // tables of whichever kernel execC2C runs for n (not 2^k >= 32)
     int resolve(int kind, uint32_t n, int* e, int* cta) const;
     int execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                     float scale, void* stream, void* work);

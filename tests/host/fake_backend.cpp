@@ -203,6 +203,16 @@ int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool 
     return 0;
 }
 
+int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
+                const void*, void*) {
+    if (!mixedRadix((uint32_t)plan.n, nullptr)) return 1;
+    if (int r = launch()) return r;
+    const uint32_t n = (uint32_t)plan.n;
+    for (uint64_t b = 0; b < batch; ++b)
+        dft((const float*)in + b * 2 * n, (float*)out + b * 2 * n, n, inverse ? 1 : -1, scale);
+    return 0;
+}
+
 bool hasStft(uint32_t n) { return n >= kStftMinN && n <= kStftMaxN && !(n & (n - 1)); }
 int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal,
                uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,

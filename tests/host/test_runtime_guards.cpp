@@ -230,7 +230,8 @@ int main(int argc, char** argv) {
     CHECK(plan->execC2C(nullptr, dummy, 64, 1, -1, 1.f, nullptr) == -8);
     CHECK(plan->execC2C(dummy, dummy, 64, 0, -1, 1.f, nullptr) == -8);
     CHECK(plan->execC2C(dummy, dummy, 64, 1, 0, 1.f, nullptr) == -8);
-    CHECK(plan->execC2C(dummy, dummy, 9000, 1, -1, 1.f, nullptr) == -8);   // above the Bluestein envelope
+    CHECK(plan->execC2C(dummy, dummy, 9001, 1, -1, 1.f, nullptr) == -8);   // prime, above the Bluestein envelope
+    CHECK(plan->execC2C(dummy, dummy, 12348, 1, -1, 1.f, nullptr) == -8);  // 2^2 3^2 7^3: 7-smooth, above 12288
     CHECK(plan->execC2C(dummy, dummy, 1, 1, -1, 1.f, nullptr) == -8);
     CHECK(plan->execC2C(dummy, dummy, 131072, 1, -1, 1.f, nullptr) == -8);
     CHECK(plan->execR2C(dummy, dummy, 32, 1, 1.f, 1.f, nullptr) == -8);
@@ -434,7 +435,7 @@ int main(int argc, char** argv) {
         CHECK(plan->execC2C2D(d, d, 16, 64, 1, -1, 1.f, nullptr) == -8);      // ny below 32
         CHECK(plan->execC2C2D(d, d, 8192, 64, 1, -1, 1.f, nullptr) == -8);    // ny above 4096
         CHECK(plan->execC2C2D(d, d, 48, 64, 1, -1, 1.f, nullptr) == -8);      // ny not a power of two
-        CHECK(plan->execC2C2D(d, d, 32, 9000, 1, -1, 1.f, nullptr) == -8);    // nx beyond every row kernel
+        CHECK(plan->execC2C2D(d, d, 32, 9001, 1, -1, 1.f, nullptr) == -8);    // nx beyond every row kernel
         CHECK(plan->execC2C2D(d, d, 4096, 64, 1u << 20, -1, 1.f, nullptr) == -8);   // batch*ny > 2^32-1
         CHECK(plan->execC2CAxis(d, d, 32, 0, 3, -1, 1.f, nullptr) == -8);
         CHECK(plan->execC2CAxis(d, d, 32, 1, 0, -1, 1.f, nullptr) == -8);
@@ -554,7 +555,7 @@ int main(int argc, char** argv) {
         const int allocBefore = fake::allocations, copiesBefore = fake::copies, launchBefore = fake::launches;
         CHECK(plan->runMany(nullptr, 1) == -8);
         CHECK(plan->runMany(reqs, 0) == -8);
-        const bfly::HostRequest bad1[] = {reqs[0], {a.data(), oa.data(), 9000, 1, -1, 1.f}};
+        const bfly::HostRequest bad1[] = {reqs[0], {a.data(), oa.data(), 9001, 1, -1, 1.f}};
         const bfly::HostRequest bad2[] = {reqs[0], {a.data(), oa.data(), 64, 1, 0, 1.f}};
         const bfly::HostRequest bad3[] = {reqs[0], {nullptr, oa.data(), 64, 1, -1, 1.f}};
         const bfly::HostRequest bad4[] = {reqs[0], {a.data(), oa.data(), 64, 0, -1, 1.f}};

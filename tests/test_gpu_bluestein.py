@@ -12,7 +12,8 @@ import oracle.fft_oracle as O
 
 pytestmark = pytest.mark.gpu
 
-LENGTHS = [2, 3, 5, 7, 12, 100, 127, 243, 1000, 1023, 1536, 3000, 4095, 5000, 6561, 8191]
+# lengths with a prime factor above 7 (7-smooth lengths run the mixed-radix kernel)
+LENGTHS = [11, 13, 17, 22, 26, 97, 127, 209, 1001, 1023, 1331, 2047, 3001, 4095, 5003, 6553, 8191]
 
 
 @pytest.mark.parametrize("n", LENGTHS)
@@ -35,8 +36,8 @@ def test_bluestein_matches_fp64(plan, cuda, n, direction):
 def test_bluestein_known_answers(plan, cuda):
     """Impulse at p -> exp(-2*pi*i*p*k/n); constant -> n at bin 0; in place equals out of place."""
     import torch
-    n = 1000
-    pos = [0, 1, 7, 499, 999]
+    n = 1001
+    pos = [0, 1, 7, 499, 1000]
     x = torch.zeros(len(pos) + 1, n, dtype=torch.complex64, device=cuda)
     for r, p in enumerate(pos):
         x[r, p] = 1.0
@@ -57,7 +58,7 @@ def test_bluestein_known_answers(plan, cuda):
 
 def test_bluestein_large_batch_round_trip(plan, cuda):
     import torch
-    n, batch = 3000, 1 << 14
+    n, batch = 3001, 1 << 14
     g = torch.Generator(device=cuda).manual_seed(3)
     a = torch.randn(batch, n, dtype=torch.complex64, device=cuda, generator=g)
     fa = torch.empty_like(a)
@@ -74,14 +75,14 @@ def test_bluestein_large_batch_round_trip(plan, cuda):
 def test_bluestein_torch_layer_and_autograd(cuda):
     import torch
     import bfly
-    x0 = torch.randn(4, 360, dtype=torch.complex64, device=cuda)
+    x0 = torch.randn(4, 374, dtype=torch.complex64, device=cuda)
     for norm in (None, "ortho", "forward"):
         ref = torch.fft.fft(x0, norm=norm)
         got = bfly.fft(x0, norm=norm)
         assert (torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)).item() <= 3e-6
         back = bfly.ifft(got, norm=norm)
         assert (torch.linalg.vector_norm(back - x0) / torch.linalg.vector_norm(x0)).item() <= 4e-6
-    w = torch.rand(4, 360, device=cuda)
+    w = torch.rand(4, 374, device=cuda)
     xa = x0.clone().requires_grad_(True)
     xb = x0.clone().requires_grad_(True)
     (w * bfly.fft(xa).abs() ** 2).sum().backward()
@@ -92,7 +93,7 @@ def test_bluestein_torch_layer_and_autograd(cuda):
 def test_bluestein_in_2d_rows(plan, cuda):
     """A 2-D transform whose rows have a non-power-of-two length (columns stay power of two)."""
     import torch
-    ny, nx = 64, 100
+    ny, nx = 64, 110
     x = torch.randn(2, ny, nx, dtype=torch.complex64, device=cuda)
     y = torch.empty_like(x)
     assert plan.exec_c2c_2d(x.data_ptr(), y.data_ptr(), ny, nx, 2, -1, 1.0, 0) == 0
@@ -103,6 +104,6 @@ def test_bluestein_in_2d_rows(plan, cuda):
 
 def test_bluestein_guards(plan, cuda):
     import torch
-    x = torch.zeros(2, 9000, dtype=torch.complex64, device=cuda)
-    assert plan.exec_c2c(x.data_ptr(), x.data_ptr(), 9000, 1, -1, 1.0, 0) == -8   # above 8192
+    x = torch.zeros(2, 9001, dtype=torch.complex64, device=cuda)
+    assert plan.exec_c2c(x.data_ptr(), x.data_ptr(), 9001, 1, -1, 1.0, 0) == -8   # prime, above 8192
     assert plan.exec_c2c(x.data_ptr(), x.data_ptr(), 1, 1, -1, 1.0, 0) == -8

@@ -46,7 +46,7 @@ def test_run_many_guards(plan):
     x = np.zeros((2, 128), dtype=np.float32)
     y = np.zeros_like(x)
     assert plan.run_many([]) == -8
-    assert plan.run_many([(x, y, 64, 2), (x, y, 9000, 1)]) == -8
+    assert plan.run_many([(x, y, 64, 2), (x, y, 9001, 1)]) == -8
     assert plan.run_many([(x, y, 64, 2, 0, 1.0)]) == -8
 
 
