@@ -104,37 +104,63 @@ int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool 
                     const void* tw, const void* chirp, const void* filt, void* stream);
 
 // Mixed-radix C2C for 7-smooth lengths n = 2^a 3^b 5^c 7^d in [2, kMixedMaxN]: Stockham passes
-// of radix 16, 8, 4, 2, 7, 5, 3 (in that order) through shared memory, one kernel; tw = W_n^m,
-// m < n (linear table of n entries).  mixedRadix fills the pass list (false when n is not
-// 7-smooth or out of range); ns[p] = product of the radices before pass p.
+// through shared memory in one kernel, radices 16, 8, 4, 2 and the odd / composite radices
+// 3, 5, 7, 9 (3x3), 6, 10, 14 (2 x odd), 12 (4x3), 15 (3x5).  mixedRadix picks the passes: 16s
+// for the power-of-two part, then 15s and 9s, then the remaining odd primes, each paired with one
+// or two of the leftover factors 2 (6, 10, 14, 12), then the leftover power of two.
+// ns[p] = product of the radices before pass p; pass p >= 1 reads its twiddles W_(Ns R)^(k r)
+// at tw[twoff[p] + (r-1) Ns + k], r < R, k < Ns (twsize entries, built by buildMixedTwiddles).
 constexpr uint32_t kMixedMaxN = 12288;
 constexpr int kMixedMaxPasses = 16;
 struct MixedRadix {
-    int n = 0, passes = 0;
+    int n = 0, passes = 0, twsize = 0;
     int radix[kMixedMaxPasses] = {};
     int ns[kMixedMaxPasses] = {};
+    int twoff[kMixedMaxPasses] = {};
 };
 inline bool mixedRadix(uint32_t n, MixedRadix* m) {
     if (n < 2 || n > kMixedMaxN) return false;
+    int e[4] = {0, 0, 0, 0};   // exponents of 2, 3, 5, 7
     uint32_t rest = n;
-    MixedRadix r;
-    r.n = (int)n;
-    auto push = [&](int radix) {
-        r.ns[r.passes] = r.passes ? r.ns[r.passes - 1] * r.radix[r.passes - 1] : 1;
-        r.radix[r.passes++] = radix;
-        rest /= (uint32_t)radix;
-    };
-    while (rest % 16 == 0) push(16);
-    if (rest % 8 == 0) push(8);
-    if (rest % 4 == 0) push(4);
-    if (rest % 2 == 0) push(2);
-    static constexpr int kOdd[3] = {7, 5, 3};
-    for (int p : kOdd)
-        while (rest % (uint32_t)p == 0) push(p);
+    static constexpr uint32_t kPrime[4] = {2, 3, 5, 7};
+    for (int i = 0; i < 4; ++i)
+        while (rest % kPrime[i] == 0) {
+            rest /= kPrime[i];
+            ++e[i];
+        }
     if (rest != 1) return false;
-    if (m) *m = r;
+    if (!m) return true;
+    // k16 passes of radix 16 first; the rest as below.  Every k16 from the most to none is tried
+    // and the fewest passes kept (n = 10000: 10^4 rather than 16 5^4).
+    auto build = [&](int k16) {
+        MixedRadix r;
+        r.n = (int)n;
+        int f[4] = {e[0] - 4 * k16, e[1], e[2], e[3]};
+        auto push = [&](int radix) {
+            r.ns[r.passes] = r.passes ? r.ns[r.passes - 1] * r.radix[r.passes - 1] : 1;
+            r.twoff[r.passes] = r.twsize;
+            if (r.passes) r.twsize += (radix - 1) * r.ns[r.passes];
+            r.radix[r.passes++] = radix;
+        };
+        for (int i = 0; i < k16; ++i) push(16);
+        for (; f[1] >= 1 && f[2] >= 1; --f[1], --f[2]) push(15);
+        for (; f[1] >= 2; f[1] -= 2) push(9);
+        for (; f[3] >= 1; --f[3]) push(f[0] >= 1 ? (--f[0], 14) : 7);
+        for (; f[2] >= 1; --f[2]) push(f[0] >= 1 ? (--f[0], 10) : 5);
+        for (; f[1] >= 1; --f[1]) push(f[0] >= 2 ? (f[0] -= 2, 12) : f[0] >= 1 ? (--f[0], 6) : 3);
+        for (; f[0] >= 4; f[0] -= 4) push(16);
+        if (f[0] >= 1) push(1 << f[0]);
+        return r;
+    };
+    MixedRadix best = build(e[0] / 4);
+    for (int k16 = e[0] / 4 - 1; k16 >= 0; --k16) {
+        const MixedRadix r = build(k16);
+        if (r.passes < best.passes) best = r;
+    }
+    *m = best;
     return true;
 }
+int buildMixedTwiddles(void* tw, const MixedRadix& plan, void* stream);   // FP64 on the device
 int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
                 const void* tw, void* stream);
 

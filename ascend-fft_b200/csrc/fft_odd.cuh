@@ -1,4 +1,5 @@
-// Small odd-length DFTs in registers (3, 5, 7), natural order in and out, forward sign
+// Small odd-length DFTs in registers (3, 5, 7, 9) and Good-Thomas composites (6, 10, 12, 14,
+// 15), natural order in and out, forward sign
 // exp(-2*pi*i*j*k/R) (INV flips it), and their DFT<R, INV> specialisations for the radix
 // passes.  Each pairs x[m] with x[R-m]: t = x[m] + x[R-m], d = x[m] - x[R-m], then
 //   X[k]   = x0 + sum_m cos(2 pi k m / R) t_m  -/+  i sum_m sin(2 pi k m / R) d_m
@@ -66,6 +67,68 @@ __device__ __forceinline__ void dft7(float2* x) {
     x[4] = csub(a3, b3);
 }
 
+// 9 = 3 x 3 Cooley-Tukey: j = 3 j1 + j2, k = k1 + 3 k2, inner twiddles W_9^(j2 k1).
+template <bool INV>
+__device__ __forceinline__ void dft9(float2* v) {
+    constexpr float kC1 = 0.766044443118978035f, kS1 = 0.642787609686539326f;    // 2pi/9
+    constexpr float kC2 = 0.173648177666930349f, kS2 = 0.984807753012208060f;    // 4pi/9
+    constexpr float kC4 = -0.939692620785908384f, kS4 = 0.342020143325668734f;   // 8pi/9
+#pragma unroll
+    for (int j2 = 0; j2 < 3; ++j2) dft3<INV>(v[j2], v[3 + j2], v[6 + j2]);   // v[3 k1 + j2]
+    const float2 w1 = make_float2(kC1, -kS1), w2 = make_float2(kC2, -kS2), w4 = make_float2(kC4, -kS4);
+    v[4] = cmul<INV>(v[4], w1);   // k1 = 1, j2 = 1
+    v[5] = cmul<INV>(v[5], w2);   // k1 = 1, j2 = 2
+    v[7] = cmul<INV>(v[7], w2);   // k1 = 2, j2 = 1
+    v[8] = cmul<INV>(v[8], w4);   // k1 = 2, j2 = 2
+    float2 y[9];
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+        float2 a = v[3 * k1], b = v[3 * k1 + 1], c = v[3 * k1 + 2];
+        dft3<INV>(a, b, c);
+        y[k1] = a;
+        y[k1 + 3] = b;
+        y[k1 + 6] = c;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v[k] = y[k];
+}
+
+// x with (a * x) mod m == 1 (gcd(a, m) = 1; 0 for m = 1), at compile time.
+__host__ __device__ constexpr int mod_inv(int a, int m) {
+    for (int x = 1; x < m; ++x)
+        if ((a * x) % m == 1) return x;
+    return 0;
+}
+
+template <int R, bool INV> struct DFT;
+
+// R = A*B with gcd(A, B) = 1 by Good-Thomas, no inner twiddles: input j = CRT(j1, j2)
+// (j = j1 mod A, j = j2 mod B), output k = (B k1 + A k2) mod R.
+template <int A, int B, bool INV>
+__device__ __forceinline__ void dft_pfa(float2* v) {
+    constexpr int R = A * B;
+    constexpr int U = B * mod_inv(B % A, A), V = A * mod_inv(A % B, B);
+    float2 y[R];   // y[j1 B + k2]
+#pragma unroll
+    for (int j1 = 0; j1 < A; ++j1) {
+        float2 c[B];
+#pragma unroll
+        for (int j2 = 0; j2 < B; ++j2) c[j2] = v[(j1 * U + j2 * V) % R];
+        DFT<B, INV>::run(c);
+#pragma unroll
+        for (int k2 = 0; k2 < B; ++k2) y[j1 * B + k2] = c[k2];
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) {
+        float2 c[A];
+#pragma unroll
+        for (int j1 = 0; j1 < A; ++j1) c[j1] = y[j1 * B + k2];
+        DFT<A, INV>::run(c);
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) v[(B * k1 + A * k2) % R] = c[k1];
+    }
+}
+
 template <bool INV> struct DFT<3, INV> {
     static __device__ __forceinline__ void run(float2* v) { dft3<INV>(v[0], v[1], v[2]); }
 };
@@ -74,6 +137,24 @@ template <bool INV> struct DFT<5, INV> {
 };
 template <bool INV> struct DFT<7, INV> {
     static __device__ __forceinline__ void run(float2* v) { dft7<INV>(v); }
+};
+template <bool INV> struct DFT<9, INV> {
+    static __device__ __forceinline__ void run(float2* v) { dft9<INV>(v); }
+};
+template <bool INV> struct DFT<6, INV> {
+    static __device__ __forceinline__ void run(float2* v) { dft_pfa<2, 3, INV>(v); }
+};
+template <bool INV> struct DFT<10, INV> {
+    static __device__ __forceinline__ void run(float2* v) { dft_pfa<2, 5, INV>(v); }
+};
+template <bool INV> struct DFT<12, INV> {
+    static __device__ __forceinline__ void run(float2* v) { dft_pfa<4, 3, INV>(v); }
+};
+template <bool INV> struct DFT<14, INV> {
+    static __device__ __forceinline__ void run(float2* v) { dft_pfa<2, 7, INV>(v); }
+};
+template <bool INV> struct DFT<15, INV> {
+    static __device__ __forceinline__ void run(float2* v) { dft_pfa<3, 5, INV>(v); }
 };
 
 }  // namespace dev

@@ -1,12 +1,14 @@
 // Mixed-radix C2C for 7-smooth lengths (n = 2^a 3^b 5^c 7^d up to kMixedMaxN), one HBM pass.
 // Stockham autosort: pass p of radix R over Ns = R_0 ... R_(p-1) takes butterfly j < n/R,
-// k = j mod Ns, inputs x[j + r n/R], twiddles W_(Ns R)^(k r) = W_n^(k r n/(Ns R)) (one FP64-built
-// table of W_n^m, m < n, indexed without a modulo since k r n/(Ns R) < n), an R-point DFT in
-// registers and outputs at (j - k) R + k + r Ns.  A row of n values lives in two shared buffers
-// (ping-pong); the first pass reads HBM directly (coalesced over j), the last writes HBM
-// directly (Ns = n/R there, so the store index is j + r n/R, coalesced too).  T = ceil(n/8)
-// threads per row, each taking butterflies j = t, t + T, ...; rows packed to ~256 threads.
-// The radix list is a kernel argument, so one kernel serves every such length.
+// k = j mod Ns, inputs x[j + r n/R], twiddles W_(Ns R)^(k r) from the pass's slice of an
+// FP64-built table (entry (r-1) Ns + k: consecutive threads read consecutive entries), an
+// R-point DFT in registers (radix 2..16, odd and Good-Thomas composite radices included) and
+// outputs at (j - k) R + k + r Ns.  A row of n values lives in two shared buffers (ping-pong);
+// the first pass reads HBM directly (coalesced over j), the last writes HBM directly (Ns = n/R
+// there, so the store index is j + r n/R, coalesced too).  T = min(512, ceil(n/8)) threads per
+// row, each taking butterflies j = t, t + T, ...; rows packed to ~256 threads.  k = j mod Ns
+// uses a multiply-high by ceil(2^32 / Ns) (exact for j, Ns < 2^14).  The pass list is a kernel
+// argument, so one kernel serves every such length.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,22 +24,25 @@ struct MixedArgs {
     int n, passes;
     int radix[backend::kMixedMaxPasses];
     int ns[backend::kMixedMaxPasses];
+    int twoff[backend::kMixedMaxPasses];
+    unsigned magic[backend::kMixedMaxPasses];   // ceil(2^32 / ns), pass p >= 1
 };
 
 // KIND bit 0: source is the row in HBM; bit 1: destination is the row in HBM (scaled).
+// Pass 0 (Ns = 1) has no twiddles.
 template <int R, bool INV, int KIND>
 __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float2* __restrict__ dst, int n, int Ns,
-                                           const float2* __restrict__ tw, int t, int T, float scale) {
+                                           unsigned magic, const float2* __restrict__ twp, int t, int T,
+                                           float scale) {
     const int nb = n / R;
-    const int tws = n / (Ns * R);
     for (int j = t; j < nb; j += T) {
-        const int k = j % Ns;
+        const int k = (KIND & 1) ? 0 : j - Ns * (int)__umulhi((unsigned)j, magic);
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = (KIND & 1) ? ld_stream(src + j + r * nb) : src[spad(j + r * nb)];
-        if (k) {
+        if (!(KIND & 1)) {
 #pragma unroll
-            for (int r = 1; r < R; ++r) v[r] = cmul<INV>(v[r], __ldg(tw + k * r * tws));
+            for (int r = 1; r < R; ++r) v[r] = cmul<INV>(v[r], __ldg(twp + (r - 1) * Ns + k));
         }
         DFT<R, INV>::run(v);
         const int base = (j - k) * R + k;
@@ -50,23 +55,32 @@ __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float
 }
 
 template <bool INV, int KIND>
-__device__ __forceinline__ void mixed_pass_r(int R, const float2* src, float2* dst, int n, int Ns, const float2* tw,
-                                             int t, int T, float scale) {
+__device__ __forceinline__ void mixed_pass_r(int R, const float2* src, float2* dst, int n, int Ns, unsigned magic,
+                                             const float2* twp, int t, int T, float scale) {
+#define BFLY_MP(RR) \
+    case RR: mixed_pass<RR, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale); break
     switch (R) {
-        case 16: mixed_pass<16, INV, KIND>(src, dst, n, Ns, tw, t, T, scale); break;
-        case 8: mixed_pass<8, INV, KIND>(src, dst, n, Ns, tw, t, T, scale); break;
-        case 4: mixed_pass<4, INV, KIND>(src, dst, n, Ns, tw, t, T, scale); break;
-        case 2: mixed_pass<2, INV, KIND>(src, dst, n, Ns, tw, t, T, scale); break;
-        case 7: mixed_pass<7, INV, KIND>(src, dst, n, Ns, tw, t, T, scale); break;
-        case 5: mixed_pass<5, INV, KIND>(src, dst, n, Ns, tw, t, T, scale); break;
-        default: mixed_pass<3, INV, KIND>(src, dst, n, Ns, tw, t, T, scale); break;
+        BFLY_MP(16);
+        BFLY_MP(15);
+        BFLY_MP(14);
+        BFLY_MP(12);
+        BFLY_MP(10);
+        BFLY_MP(9);
+        BFLY_MP(8);
+        BFLY_MP(7);
+        BFLY_MP(6);
+        BFLY_MP(5);
+        BFLY_MP(4);
+        BFLY_MP(3);
+        default: mixed_pass<2, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale); break;
     }
+#undef BFLY_MP
 }
 
 template <bool INV>
-__global__ void __launch_bounds__(1024) k_mixed(const float2* __restrict__ in, float2* __restrict__ out,
-                                                const float2* __restrict__ tw, MixedArgs a, uint64_t batch, int T,
-                                                int rows, int len, float scale) {
+__global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in, float2* __restrict__ out,
+                                                  const float2* __restrict__ tw, MixedArgs a, uint64_t batch, int T,
+                                                  int rows, int len, float scale) {
     extern __shared__ float2 smem[];
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
@@ -79,35 +93,69 @@ __global__ void __launch_bounds__(1024) k_mixed(const float2* __restrict__ in, f
     float2* buf1 = buf0 + len;
     for (int p = 0; p < a.passes; ++p) {
         const int R = a.radix[p], Ns = a.ns[p];
+        const unsigned mg = a.magic[p];
+        const float2* twp = tw + a.twoff[p];
         const bool first = p == 0, last = p == a.passes - 1;
         const float2* s = (p & 1) ? buf0 : buf1;   // written by pass p - 1
         float2* d = (p & 1) ? buf1 : buf0;
         if (ok) {
-            if (first && last) mixed_pass_r<INV, 3>(R, src, dst, n, Ns, tw, t, T, scale);
-            else if (first) mixed_pass_r<INV, 1>(R, src, d, n, Ns, tw, t, T, scale);
-            else if (last) mixed_pass_r<INV, 2>(R, s, dst, n, Ns, tw, t, T, scale);
-            else mixed_pass_r<INV, 0>(R, s, d, n, Ns, tw, t, T, scale);
+            if (first && last) mixed_pass_r<INV, 3>(R, src, dst, n, Ns, mg, twp, t, T, scale);
+            else if (first) mixed_pass_r<INV, 1>(R, src, d, n, Ns, mg, twp, t, T, scale);
+            else if (last) mixed_pass_r<INV, 2>(R, s, dst, n, Ns, mg, twp, t, T, scale);
+            else mixed_pass_r<INV, 0>(R, s, d, n, Ns, mg, twp, t, T, scale);
         }
         if (!last) __syncthreads();
     }
+}
+
+// tw[twoff[p] + (r-1) Ns + k] = W_(Ns R)^(k r) = W_n^(k r n / (Ns R)) in FP64, rounded once.
+static __global__ void k_tw_mixed(float2* __restrict__ tw, MixedArgs a, int total) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    int p = 1;
+    while (p + 1 < a.passes && a.twoff[p + 1] <= i) ++p;
+    const int local = i - a.twoff[p], Ns = a.ns[p], R = a.radix[p];
+    const int r = local / Ns + 1, k = local % Ns;
+    const long long m = (long long)k * r * (a.n / (Ns * R));
+    double s, c;
+    sincospi(-2.0 * (double)m / (double)a.n, &s, &c);
+    tw[i] = make_float2((float)c, (float)s);
 }
 
 }  // namespace dev
 
 namespace backend {
 
-int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
-                const void* tw, void* stream) {
-    if (plan.n < 2 || plan.passes < 1 || plan.passes > kMixedMaxPasses || (uint32_t)plan.n > kMixedMaxN)
-        return (int)cudaErrorInvalidValue;
-    dev::MixedArgs a;
+namespace {
+dev::MixedArgs mixedArgs(const MixedRadix& plan) {
+    dev::MixedArgs a{};
     a.n = plan.n;
     a.passes = plan.passes;
     for (int p = 0; p < kMixedMaxPasses; ++p) {
         a.radix[p] = plan.radix[p];
         a.ns[p] = plan.ns[p];
+        a.twoff[p] = plan.twoff[p];
+        a.magic[p] = plan.ns[p] > 1 ? (unsigned)((0x100000000ull + plan.ns[p] - 1) / (unsigned long long)plan.ns[p]) : 0u;
     }
-    const int T = std::min(1024, (plan.n + 7) / 8);
+    return a;
+}
+bool mixedValid(const MixedRadix& plan) {
+    return plan.n >= 2 && (uint32_t)plan.n <= kMixedMaxN && plan.passes >= 1 && plan.passes <= kMixedMaxPasses;
+}
+}  // namespace
+
+int buildMixedTwiddles(void* tw, const MixedRadix& plan, void* stream) {
+    if (!mixedValid(plan)) return (int)cudaErrorInvalidValue;
+    if (plan.twsize == 0) return 0;
+    dev::k_tw_mixed<<<(plan.twsize + 255) / 256, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<float2*>(tw), mixedArgs(plan), plan.twsize);
+    return (int)cudaGetLastError();
+}
+
+int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
+                const void* tw, void* stream) {
+    if (!mixedValid(plan)) return (int)cudaErrorInvalidValue;
+    const int T = std::min(512, (plan.n + 7) / 8);
     const int rows = std::max(1, 256 / T);
     const int len = dev::spad(plan.n - 1) + 1;
     const int smem = rows * 2 * len * 8;
@@ -120,8 +168,8 @@ int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batc
     const uint64_t grid = (batch + rows - 1) / rows;
     if (grid > 0x7fffffffull) return (int)cudaErrorInvalidValue;
     fn<<<(unsigned)grid, T * rows, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw), a, batch, T, rows,
-        len, scale);
+        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw), mixedArgs(plan),
+        batch, T, rows, len, scale);
     return (int)cudaGetLastError();
 }
 

@@ -373,7 +373,11 @@ struct Plan::Impl {
     };
     std::map<uint32_t, Chirp> bluestein;   // non-power-of-two n -> Bluestein tables
     std::map<uint32_t, void*> dftSmall;    // A -> W_A^m, m < A (prime-factor kernels)
-    std::map<uint32_t, void*> mixedTw;     // 7-smooth n -> W_n^m, m < n (mixed-radix kernel)
+    struct Mixed {
+        backend::MixedRadix plan;   // passes of the mixed-radix kernel
+        void* tw = nullptr;         // their twiddles (plan.twsize entries)
+    };
+    std::map<uint32_t, Mixed> mixed;   // 7-smooth n served by the mixed-radix kernel
 };
 
 Plan::Plan(Candidate c) : cand_(std::move(c)) {}
@@ -405,8 +409,8 @@ Plan::~Plan() {
         if (t) backend::release(t);
     for (auto& kv : impl_->dftSmall)
         if (kv.second) backend::release(kv.second);
-    for (auto& kv : impl_->mixedTw)
-        if (kv.second) backend::release(kv.second);
+    for (auto& kv : impl_->mixed)
+        if (kv.second.tw) backend::release(kv.second.tw);
     for (auto& kv : impl_->bluestein) {
         if (kv.second.chirp) backend::release(kv.second.chirp);
         if (kv.second.filt) backend::release(kv.second.filt);
@@ -561,15 +565,15 @@ int Plan::preparePfa(uint32_t n) {
 }
 
 int Plan::prepareMixed(uint32_t n) {
-    if (!backend::mixedRadix(n, nullptr)) return -1;
-    if (impl_->mixedTw.count(n)) return 0;
-    void* w = nullptr;
-    if (backend::alloc(&w, (size_t)n * 8)) return -1;
-    if (backend::buildLinearTwiddles(w, (int)n, 1, n, stream_) || backend::streamSync(stream_)) {
-        backend::release(w);
+    if (impl_->mixed.count(n)) return 0;
+    Impl::Mixed m;
+    if (!backend::mixedRadix(n, &m.plan)) return -1;
+    if (backend::alloc(&m.tw, (size_t)std::max(m.plan.twsize, 1) * 8)) return -1;
+    if (backend::buildMixedTwiddles(m.tw, m.plan, stream_) || backend::streamSync(stream_)) {
+        backend::release(m.tw);
         return -1;
     }
-    impl_->mixedTw[n] = w;
+    impl_->mixed[n] = m;
     return 0;
 }
 
@@ -638,10 +642,10 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
             return -5;
         return 0;
     }
-    backend::MixedRadix mr;
-    if ((!pow2(n) || n < kMinN) && backend::mixedRadix(n, &mr)) {   // other 7-smooth lengths
+    if ((!pow2(n) || n < kMinN) && backend::mixedRadix(n, nullptr)) {   // other 7-smooth lengths
         if (prepareMixed(n)) return -2;
-        if (backend::launchMixed(dIn, dOut, mr, batch, inv, scale, impl_->mixedTw[n], s)) return -5;
+        const auto& m = impl_->mixed[n];
+        if (backend::launchMixed(dIn, dOut, m.plan, batch, inv, scale, m.tw, s)) return -5;
         return 0;
     }
     if (!pow2(n) || n < kMinN) {   // Bluestein: one kernel on the padded power-of-two length

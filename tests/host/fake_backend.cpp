@@ -203,6 +203,7 @@ int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool 
     return 0;
 }
 
+int buildMixedTwiddles(void*, const MixedRadix& plan, void*) { return plan.passes > 0 ? launch() : 1; }
 int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
                 const void*, void*) {
     if (!mixedRadix((uint32_t)plan.n, nullptr)) return 1;
