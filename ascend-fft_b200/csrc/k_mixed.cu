@@ -5,8 +5,8 @@
 // R-point DFT in registers (radix 2..16, odd and Good-Thomas composite radices included) and
 // outputs at (j - k) R + k + r Ns.  A row of n values lives in two shared buffers (ping-pong);
 // the first pass reads HBM directly (coalesced over j), the last writes HBM directly (Ns = n/R
-// there, so the store index is j + r n/R, coalesced too).  T = min(512, ceil(n/8)) threads per
-// row, each taking butterflies j = t, t + T, ...; rows packed to ~256 threads.  k = j mod Ns
+// there, so the store index is j + r n/R, coalesced too).  T = min(512, ceil(n / R_max)) threads
+// per row, each taking butterflies j = t, t + T, ...; max(1, 224 / T) rows per CTA.  k = j mod Ns
 // uses a multiply-high by ceil(2^32 / Ns) (exact for j, Ns < 2^14).  The pass list is a kernel
 // argument, so one kernel serves every such length.
 #include <cuda_runtime.h>
@@ -26,20 +26,33 @@ struct MixedArgs {
     int ns[backend::kMixedMaxPasses];
     int twoff[backend::kMixedMaxPasses];
     unsigned magic[backend::kMixedMaxPasses];   // ceil(2^32 / ns), pass p >= 1
+    int pad0;          // the buffer pass 0 writes: element i at i + i / pad0 (pad0 = 0: at i)
+    unsigned magic0;   // ceil(2^32 / pad0)
 };
 
-// KIND bit 0: source is the row in HBM; bit 1: destination is the row in HBM (scaled).
+// Shared-memory position of element i: the buffer pass 0 writes is padded by one slot every
+// pad0 elements (pad0 = R_0 when even, so its stride-R_0 stores hit distinct banks); the
+// others use spad.
+template <bool PASS0_BUF>
+__device__ __forceinline__ int mixed_at(int i, int pad0, unsigned magic0) {
+    if constexpr (PASS0_BUF) return pad0 ? i + (int)__umulhi((unsigned)i, magic0) : i;
+    else return spad(i);
+}
+
+// KIND bit 0: source is the row in HBM (pass 0, which writes the pass-0 buffer); bit 1:
+// destination is the row in HBM (scaled); bit 2: source is the pass-0 buffer (pass 1).
 // Pass 0 (Ns = 1) has no twiddles.
 template <int R, bool INV, int KIND>
 __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float2* __restrict__ dst, int n, int Ns,
                                            unsigned magic, const float2* __restrict__ twp, int t, int T,
-                                           float scale) {
+                                           float scale, int pad0, unsigned magic0) {
     const int nb = n / R;
     for (int j = t; j < nb; j += T) {
         const int k = (KIND & 1) ? 0 : j - Ns * (int)__umulhi((unsigned)j, magic);
         float2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = (KIND & 1) ? ld_stream(src + j + r * nb) : src[spad(j + r * nb)];
+        for (int r = 0; r < R; ++r)
+            v[r] = (KIND & 1) ? ld_stream(src + j + r * nb) : src[mixed_at<(KIND & 4) != 0>(j + r * nb, pad0, magic0)];
         if (!(KIND & 1)) {
 #pragma unroll
             for (int r = 1; r < R; ++r) v[r] = cmul<INV>(v[r], __ldg(twp + (r - 1) * Ns + k));
@@ -49,16 +62,17 @@ __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (KIND & 2) st_stream(dst + base + r * Ns, cscale(v[r], scale));
-            else dst[spad(base + r * Ns)] = v[r];
+            else dst[mixed_at<(KIND & 1) != 0>(base + r * Ns, pad0, magic0)] = v[r];
         }
     }
 }
 
 template <bool INV, int KIND>
 __device__ __forceinline__ void mixed_pass_r(int R, const float2* src, float2* dst, int n, int Ns, unsigned magic,
-                                             const float2* twp, int t, int T, float scale) {
+                                             const float2* twp, int t, int T, float scale, int pad0,
+                                             unsigned magic0) {
 #define BFLY_MP(RR) \
-    case RR: mixed_pass<RR, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale); break
+    case RR: mixed_pass<RR, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0); break
     switch (R) {
         BFLY_MP(16);
         BFLY_MP(15);
@@ -72,7 +86,7 @@ __device__ __forceinline__ void mixed_pass_r(int R, const float2* src, float2* d
         BFLY_MP(5);
         BFLY_MP(4);
         BFLY_MP(3);
-        default: mixed_pass<2, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale); break;
+        default: mixed_pass<2, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0); break;
     }
 #undef BFLY_MP
 }
@@ -98,11 +112,15 @@ __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in,
         const bool first = p == 0, last = p == a.passes - 1;
         const float2* s = (p & 1) ? buf0 : buf1;   // written by pass p - 1
         float2* d = (p & 1) ? buf1 : buf0;
+        const int p0 = a.pad0;
+        const unsigned m0 = a.magic0;
         if (ok) {
-            if (first && last) mixed_pass_r<INV, 3>(R, src, dst, n, Ns, mg, twp, t, T, scale);
-            else if (first) mixed_pass_r<INV, 1>(R, src, d, n, Ns, mg, twp, t, T, scale);
-            else if (last) mixed_pass_r<INV, 2>(R, s, dst, n, Ns, mg, twp, t, T, scale);
-            else mixed_pass_r<INV, 0>(R, s, d, n, Ns, mg, twp, t, T, scale);
+            if (first && last) mixed_pass_r<INV, 3>(R, src, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (first) mixed_pass_r<INV, 1>(R, src, d, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (p == 1 && last) mixed_pass_r<INV, 6>(R, s, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (p == 1) mixed_pass_r<INV, 4>(R, s, d, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (last) mixed_pass_r<INV, 2>(R, s, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else mixed_pass_r<INV, 0>(R, s, d, n, Ns, mg, twp, t, T, scale, p0, m0);
         }
         if (!last) __syncthreads();
     }
@@ -155,21 +173,37 @@ int buildMixedTwiddles(void* tw, const MixedRadix& plan, void* stream) {
 int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
                 const void* tw, void* stream) {
     if (!mixedValid(plan)) return (int)cudaErrorInvalidValue;
-    const int T = std::min(512, (plan.n + 7) / 8);
-    const int rows = std::max(1, 256 / T);
-    const int len = dev::spad(plan.n - 1) + 1;
-    const int smem = rows * 2 * len * 8;
-    auto* fn = inverse ? dev::k_mixed<true> : dev::k_mixed<false>;
-    // opted in once per device at the largest row pair (n = kMixedMaxN, one row per CTA)
+    // one butterfly of the largest radix per thread and pass (more of the smaller radices)
+    int rmax = 2;
+    for (int p = 0; p < plan.passes; ++p) rmax = std::max(rmax, plan.radix[p]);
+    // measured on B200 over n = 12..12000: ceil(n / R_max) threads per row with ~200-300 threads
+    // per CTA beat n/8 threads per row, larger CTAs, and an 80-register budget
+    const int T = std::min(512, (plan.n + rmax - 1) / rmax);
+    const int rows = std::max(1, 224 / T);
     constexpr int kMaxSmem = 2 * (dev::spad((int)kMixedMaxN - 1) + 1) * 8;
     static_assert(kMaxSmem <= 227 * 1024, "two rows of the longest length fit in shared memory");
+    dev::MixedArgs args = mixedArgs(plan);
+    // pass 0 stores at stride R_0: pad its buffer every R_0 slots when R_0 is even (odd strides
+    // are conflict-free already), unless that no longer fits; pad 16 is spad's layout
+    const int r0 = plan.radix[0];
+    int len = dev::spad(plan.n - 1) + 1;
+    args.pad0 = (r0 % 2 == 0 && plan.passes > 1) ? r0 : 0;
+    if (args.pad0) {
+        const int len0 = std::max(len, plan.n + (plan.n - 1) / args.pad0 + 1);
+        if (rows * 2 * len0 * 8 <= kMaxSmem) len = len0;
+        else args.pad0 = 16;
+    }
+    args.magic0 = args.pad0 ? (unsigned)((0x100000000ull + args.pad0 - 1) / (unsigned long long)args.pad0) : 0u;
+    const int smem = rows * 2 * len * 8;
+    auto* fn = inverse ? dev::k_mixed<true> : dev::k_mixed<false>;
+    // opted in once per device at kMaxSmem (the largest row pair: n = kMixedMaxN, one row per CTA)
     if (smem > kMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMaxSmem)) return e;
     const uint64_t grid = (batch + rows - 1) / rows;
     if (grid > 0x7fffffffull) return (int)cudaErrorInvalidValue;
     fn<<<(unsigned)grid, T * rows, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw), mixedArgs(plan),
-        batch, T, rows, len, scale);
+        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw), args, batch, T,
+        rows, len, scale);
     return (int)cudaGetLastError();
 }
 
