@@ -393,7 +393,7 @@ def extra_measurements(dev, stream):
     # ---- non-power-of-two C2C, batch * n ~ 2^25: prime-factor kernel (n = A * 2^k) and
     # Bluestein (other lengths), one kernel each
     out["c2c_any_length"] = {}
-    for n in (1536, 1920, 6144, 1000, 3000, 8191):
+    for n in (1536, 1920, 6144, 360, 1000, 3000, 6561, 12000, 1001, 8191):
         b = (1 << 25) // n
         g = torch.Generator(device=dev).manual_seed(n)
         x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
@@ -402,9 +402,14 @@ def extra_measurements(dev, stream):
         ms = timed(lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh))
         gbs = 16 * n * b / ms / 1e6
         pfa = any(n % a == 0 and (n // a) & (n // a - 1) == 0 and n // a >= 16 for a in (3, 5, 9, 15))
+        m = n
+        for p in (2, 3, 5, 7):
+            while m % p == 0:
+                m //= p
+        kernel = ("prime-factor" if pfa else "mixed-radix" if m == 1 and n <= 12288
+                  else f"bluestein (padded length {1 << (2 * n - 2).bit_length()})")
         out["c2c_any_length"][f"n{n}_b{b}"] = {
-            "gbs": round(gbs, 1), "frac": round(gbs / peak, 4), "rel_l2": rel(y, x),
-            "kernel": "prime-factor" if pfa else f"bluestein (padded length {1 << (2 * n - 2).bit_length()})"}
+            "gbs": round(gbs, 1), "frac": round(gbs / peak, 4), "rel_l2": rel(y, x), "kernel": kernel}
         del x, y
     # ---- STFT (frame gather + Hann window + one-sided transform in one kernel), 4 signals of
     # 2^24 samples, centred; bytes counted per frame as the reference's dense-frame R2C proxy
@@ -675,7 +680,7 @@ def run_ours(args):
 
 def run_case(spec: str, reps: int):
     """Launch one kernel configuration `reps` times without timing (for ncu captures):
-    spec = kind:n:batch with kind in c2c, c2c_inv (any n: non-powers of two run the Bluestein
+    spec = kind:n:batch with kind in c2c, c2c_inv (any n: non-powers of two run the prime-factor, mixed-radix or Bluestein
     kernel), tc2, tc3 (tensor-core splits), r2c, c2r, cluster (long C2C on the cluster
     schedule), or ragged:grid:CAP; or cols:NY:NCOLS:MATS (column kernel), c2d:NY:NX:B (2-D),
     stft:N:HOP:LEN (4 signals, centred, Hann window), istft:N:HOP:LEN (its inverse)."""
