@@ -207,7 +207,8 @@ int launchRaggedFlat(const void* entries, int count, const void* tileMap, uint64
 // Device status word of the staged launches (nonzero: a bounded wait ran out).
 int raggedStatus(unsigned* status, bool clear);
 
-// Split-BF16 tensor-core C2C (tcgen05): n in {256, 4096}, split = 2 or 3 bf16 terms; tw is the
+// Split-BF16 tensor-core C2C (tcgen05): n a power of two in 64..4096 (radix-16 passes on the
+// tensor cores, a final radix-2/4/8 pass in fp32), split = 2 or 3 bf16 terms; tw is the
 // Stockham table of (n, 16).
 bool hasTensorVariant(uint32_t n, int split);
 size_t tensorTableBytes(int split);                            // split DFT-16 operand

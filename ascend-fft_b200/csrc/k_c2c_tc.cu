@@ -1,5 +1,7 @@
-// Split-BF16 tensor-core C2C for lengths that are powers of 16 (256, 4096): every radix-16 pass
-// is a dense complex contraction on the 5th-generation tensor cores.
+// Split-BF16 tensor-core C2C for power-of-two lengths 64..4096: every radix-16 pass is a dense
+// complex contraction on the 5th-generation tensor cores; lengths that are not powers of 16 end
+// with one radix-2/4/8 pass on the CUDA cores in fp32 (64 = 16 x 4, 128 = 16 x 8,
+// 512 = 16 x 16 x 2, 1024 = 16 x 16 x 4, 2048 = 16 x 16 x 8).
 //
 // Pass structure (Stockham, as in fft_core.cuh, one butterfly per thread): thread t owns
 // butterfly j of its row and holds the 16 (twiddled, fp32) inputs x_0..x_15.  As reals they form
@@ -91,11 +93,14 @@ k_c2c_tc(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
          const unsigned char* __restrict__ dftTable, uint64_t batch, int direction, float scale) {
     constexpr int E = 16;
     using Sd = Sched<N, E>;
-    static_assert(Sd::radix(Sd::P - 1) == 16, "length must be a power of 16");
-    constexpr int T = N / E;                      // butterflies per row = threads per row
+    constexpr int T = N / E;                      // radix-16 butterflies per row = threads per row
     constexpr int ROWS = kTcThreads / T;
+    static_assert(ROWS * T == kTcThreads, "rows fill the CTA");
     constexpr int S = smem_stride<N, E, false>();
     constexpr int P = Sd::P;
+    constexpr int RL = Sd::radix(P - 1);          // last radix: 16, or 2/4/8 on the CUDA cores
+    constexpr int PT = RL == 16 ? P : P - 1;      // passes on the tensor cores
+    static_assert(PT >= 1, "at least one radix-16 pass");
     constexpr int NPROD = SPLIT == 2 ? 3 : 6;
 
     extern __shared__ __align__(1024) unsigned char smem_tc[];
@@ -146,7 +151,7 @@ k_c2c_tc(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
             v[r] = make_float2(x.x, sgn * x.y);
         }
 #pragma unroll 1
-        for (int p = 0; p < P; ++p) {
+        for (int p = 0; p < PT; ++p) {
             const int Ns = Sd::ns(p);
             if (p > 0) {
                 const float2* twp = tw + Sd::twoff(p);
@@ -214,14 +219,32 @@ k_c2c_tc(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
                 for (int r = 0; r < 16; ++r) xr[spad(base + r * Ns)] = v[r];
                 tc_fence_before_sync();
                 __syncthreads();
+                // next pass's inputs: one radix-16 butterfly, or 16/RL radix-RL butterflies
+                // j + s T (elements r N/RL) for the final CUDA-core pass
 #pragma unroll
-                for (int r = 0; r < 16; ++r) v[r] = xr[spad(j + r * (N / 16))];
+                for (int i = 0; i < 16; ++i)
+                    v[i] = p + 1 < PT ? xr[spad(j + i * (N / 16))]
+                                      : xr[spad(j + (i / RL) * T + (i % RL) * (N / RL))];
+            }
+        }
+        if constexpr (RL < 16) {   // final radix-RL pass in fp32 (Stockham, as fft_core.cuh)
+            constexpr int Ns = N / RL;
+            const float2* twp = tw + Sd::twoff(P - 1);
+#pragma unroll
+            for (int sb = 0; sb < 16 / RL; ++sb) {
+                const int k = (j + sb * T) & (Ns - 1);
+#pragma unroll
+                for (int r = 1; r < RL; ++r)
+                    v[sb * RL + r] = cmul<false>(v[sb * RL + r], __ldg(twp + (r - 1) * Ns + k));
+                DFT<RL, false>::run(&v[sb * RL]);
             }
         }
         if (!failed && ok) {
 #pragma unroll
-            for (int r = 0; r < 16; ++r)
-                st_stream(dst + j + r * (N / 16), make_float2(v[r].x * scale, sgn * scale * v[r].y));
+            for (int i = 0; i < 16; ++i) {
+                const int idx = RL == 16 ? j + i * (N / 16) : j + (i / RL) * T + (i % RL) * (N / RL);
+                st_stream(dst + idx, make_float2(v[i].x * scale, sgn * scale * v[i].y));
+            }
         }
         // the exchange buffer and the A operand are rewritten by the next group
         tc_fence_before_sync();
@@ -273,7 +296,9 @@ static int launchTc(const void* in, void* out, uint64_t batch, bool inverse, flo
     return (int)cudaGetLastError();
 }
 
-bool hasTensorVariant(uint32_t n, int split) { return (n == 256 || n == 4096) && (split == 2 || split == 3); }
+bool hasTensorVariant(uint32_t n, int split) {
+    return n >= 64 && n <= 4096 && !(n & (n - 1)) && (split == 2 || split == 3);
+}
 
 size_t tensorTableBytes(int split) { return (size_t)split * dev::kBBytes; }
 
@@ -287,10 +312,17 @@ int buildTensorTable(void* table, int split, void* stream) {
 
 int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
                     const void* tw, const void* table, int split, void* stream) {
-    if (n == 256 && split == 2) return launchTc<256, 2>(in, out, batch, inverse, scale, tw, table, stream);
-    if (n == 256 && split == 3) return launchTc<256, 3>(in, out, batch, inverse, scale, tw, table, stream);
-    if (n == 4096 && split == 2) return launchTc<4096, 2>(in, out, batch, inverse, scale, tw, table, stream);
-    if (n == 4096 && split == 3) return launchTc<4096, 3>(in, out, batch, inverse, scale, tw, table, stream);
+#define BFLY_TC(NN)                                                                                   \
+    if (n == NN && split == 2) return launchTc<NN, 2>(in, out, batch, inverse, scale, tw, table, stream); \
+    if (n == NN && split == 3) return launchTc<NN, 3>(in, out, batch, inverse, scale, tw, table, stream);
+    BFLY_TC(64)
+    BFLY_TC(128)
+    BFLY_TC(256)
+    BFLY_TC(512)
+    BFLY_TC(1024)
+    BFLY_TC(2048)
+    BFLY_TC(4096)
+#undef BFLY_TC
     return (int)cudaErrorInvalidValue;
 }
 

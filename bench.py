@@ -284,11 +284,12 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ our arm
 def extra_measurements(dev, stream):
-    """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores vs fp32 at the
-    largest power-of-16 grid points; long C2C forward + backward (batch*n = 2^26; single pass up
-    to n = 16384, four-step above); 2-D C2C at the reference's planned 2-D / range-Doppler shapes
-    and transforms along a middle axis; non-power-of-two C2C (prime-factor, Bluestein); STFT; real transforms
-    forward + adjoint at batch 1024.  Each figure: algorithmic GB/s from CUDA
+    """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores (3 and 2 bf16
+    terms) vs fp32 at every point of the 49-point grid; long C2C forward + backward (batch*n =
+    2^26; single pass up to n = 16384, four-step above); 2-D C2C at the reference's planned 2-D /
+    range-Doppler shapes and transforms along a middle axis; non-power-of-two C2C (prime-factor,
+    mixed-radix, Bluestein); STFT and inverse STFT; real transforms forward + adjoint at batch
+    1024.  Each figure: algorithmic GB/s from CUDA
     events on `stream` around one replay of a CUDA graph holding 20 launches (after 3 warm-up
     launches), and the error against FP64 on sampled rows."""
     import torch
@@ -325,8 +326,8 @@ def extra_measurements(dev, stream):
         return O.rel_l2_rows(y[idx].cpu().numpy(), ref)
 
     out = {"split_bf16": {}, "long_fwd_bwd": {}, "real_fwd_adjoint": {}}
-    # ---- split-BF16 tensor cores vs plain fp32
-    for n, b in ((4096, 4096), (256, 4096)):
+    # ---- split-BF16 tensor cores vs plain fp32 at every point of the 49-point grid
+    for n, b in ((n, b) for n in GRID_N for b in GRID_B):
         g = torch.Generator(device=dev).manual_seed(grid_seed(n, b))
         x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
         y = torch.empty_like(x)

@@ -252,7 +252,8 @@ public:
 
     // Split-BF16 tensor-core C2C (5th-generation tensor cores, fp32 accumulate): every radix-16
     // pass is a dense contraction with the DFT-16 matrix, operands split into `splitTerms` = 2
-    // (hi+lo, 3 products) or 3 (hi+mid+lo, 6 products) bf16 terms.  n in {256, 4096}.
+    // (hi+lo, 3 products) or 3 (hi+mid+lo, 6 products) bf16 terms.  n a power of two in
+    // 64..4096 (radix-16 passes on the tensor cores, a final radix-2/4/8 pass in fp32).
     int execC2CTensor(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,
                       float scale, int splitTerms, void* stream);
     // Device status of the tensor-core launches: 0, or 1 when a bounded MMA wait ran out.

@@ -189,7 +189,8 @@ int bfly_plan_exec_c2r_async(bfly_plan* plan, const void* d_in, void* d_out, uin
 /* New: split-BF16 tensor-core C2C on the 5th-generation tensor cores (tcgen05, fp32
  * accumulate in tensor memory): each radix-16 pass is a dense contraction with the DFT-16
  * matrix; operands split into split_terms = 2 (hi+lo, 3 products) or 3 (hi+mid+lo, 6 products)
- * bf16 terms.  n in {256, 4096}; direction -1 / +1; output times scale; asynchronous on
+ * bf16 terms.  n a power of two in 64..4096 (radix-16 passes on the tensor cores, a final
+ * radix-2/4/8 pass in fp32 when n is not a power of 16); direction -1 / +1; output times scale; asynchronous on
  * `stream`.  The reference has no counterpart (its Cube-unit probe src/ascendc/cube_probe.cpp
  * never reached a usable matrix unit). */
 int bfly_plan_exec_c2c_tc_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,

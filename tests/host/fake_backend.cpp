@@ -333,7 +333,9 @@ int launchRaggedFlat(const void* entries, int count, const void*, uint64_t tiles
     return launchRagged(entries, count, tiles, 0, s);
 }
 
-bool hasTensorVariant(uint32_t n, int split) { return (n == 256 || n == 4096) && (split == 2 || split == 3); }
+bool hasTensorVariant(uint32_t n, int split) {
+    return n >= 64 && n <= 4096 && !(n & (n - 1)) && (split == 2 || split == 3);
+}
 size_t tensorTableBytes(int split) { return (size_t)split * 2048; }
 int buildTensorTable(void*, int, void*) { return launch(); }
 int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
