@@ -212,7 +212,7 @@ class Plan:
 
     def exec_c2c_tc(self, d_in: int, d_out: int, n: int, batch: int, direction: int = -1,
                     scale: float = 1.0, split_terms: int = 3, stream: int = 0) -> int:
-        """Split-BF16 tensor-core C2C (n = 256 or 4096; 2 or 3 bf16 terms)."""
+        """Split-BF16 tensor-core C2C (n a power of two in 64..4096; 2 or 3 bf16 terms)."""
         return self._lib.bfly_plan_exec_c2c_tc_async(self._h, d_in, d_out, n, batch, direction, scale,
                                                      split_terms, stream or None)
 

@@ -276,7 +276,7 @@ class _IRFFT(torch.autograd.Function):
 
 
 def c2c_tensor(x: torch.Tensor, direction: int = -1, scale: float = 1.0, split_terms: int = 3) -> torch.Tensor:
-    """Split-BF16 tensor-core C2C (n = 256 or 4096) on torch's current stream."""
+    """Split-BF16 tensor-core C2C (n a power of two in 64..4096) on torch's current stream."""
     _need_cuda(x, torch.complex64, "c2c_tensor")
     x = x.contiguous()
     n = x.shape[-1]
