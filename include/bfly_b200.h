@@ -127,11 +127,11 @@ int bfly_plan_run_c2c_long(bfly_plan* plan, const float* in, float* out, uint32_
  * synchronising.  The first call for a length builds
  * its twiddle tables (and the four-step workspace) and synchronises the context stream once;
  * make it before any stream capture. */
-/* C2C, power-of-two n in [32, 65536], n = A*2^k (A in {3, 5, 9, 15}, 2^k >= 16, n <= 12288) by
- * the prime-factor mapping in one kernel, or any n in [2, 8192] (the other non-powers of two
- * and 2..16 by Bluestein's algorithm in one kernel; the reference supports powers of two only,
- * docs/reference/support.md:14); direction -1 forward / +1 inverse; output multiplied by
- * scale. */
+/* C2C, power-of-two n in [32, 65536]; n = A*2^k (A in {3, 5, 9, 15}, 2^k >= 16, n <= 12288) by
+ * the prime-factor mapping in one kernel; other n = 2^a 3^b 5^c 7^d <= 12288 (2..16 included) by
+ * mixed-radix Stockham passes in one kernel; any other n in [2, 8192] by Bluestein's algorithm
+ * in one kernel (the reference supports powers of two only, docs/reference/support.md:14);
+ * direction -1 forward / +1 inverse; output multiplied by scale. */
 int bfly_plan_exec_c2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, int direction, float scale, void* stream);
 /* New: 2-D C2C over [batch][ny][nx] complex (rows of nx contiguous): nx-point row transforms
