@@ -103,11 +103,12 @@ int buildBluesteinTables(void* chirp, void* filt, void* scratch, uint32_t n, voi
 int launchBluestein(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
                     const void* tw, const void* chirp, const void* filt, void* stream);
 
-// Mixed-radix C2C for 7-smooth lengths n = 2^a 3^b 5^c 7^d in [2, kMixedMaxN]: Stockham passes
-// through shared memory in one kernel, radices 16, 8, 4, 2 and the odd / composite radices
-// 3, 5, 7, 9 (3x3), 6, 10, 14 (2 x odd), 12 (4x3), 15 (3x5).  mixedRadix picks the passes: 16s
+// Mixed-radix C2C for 13-smooth lengths n = 2^a 3^b 5^c 7^d 11^e 13^f in [2, kMixedMaxN]:
+// Stockham passes through shared memory in one kernel, radices 16, 8, 4, 2 and the odd /
+// composite radices 3, 5, 7, 9 (3x3), 11, 13, 6, 10, 14 (2 x odd), 12 (4x3), 15 (3x5).  mixedRadix picks the passes: 16s
 // for the power-of-two part, then 15s and 9s, then the remaining odd primes, each paired with one
-// or two of the leftover factors 2 (6, 10, 14, 12), then the leftover power of two.
+// or two of the leftover factors 2 (6, 10, 14, 12), then 11s and 13s, then the leftover power
+// of two.
 // ns[p] = product of the radices before pass p; pass p >= 1 reads its twiddles W_(Ns R)^(k r)
 // at tw[twoff[p] + (r-1) Ns + k], r < R, k < Ns (twsize entries, built by buildMixedTwiddles).
 constexpr uint32_t kMixedMaxN = 12288;
@@ -120,10 +121,10 @@ struct MixedRadix {
 };
 inline bool mixedRadix(uint32_t n, MixedRadix* m) {
     if (n < 2 || n > kMixedMaxN) return false;
-    int e[4] = {0, 0, 0, 0};   // exponents of 2, 3, 5, 7
+    int e[6] = {0, 0, 0, 0, 0, 0};   // exponents of 2, 3, 5, 7, 11, 13
     uint32_t rest = n;
-    static constexpr uint32_t kPrime[4] = {2, 3, 5, 7};
-    for (int i = 0; i < 4; ++i)
+    static constexpr uint32_t kPrime[6] = {2, 3, 5, 7, 11, 13};
+    for (int i = 0; i < 6; ++i)
         while (rest % kPrime[i] == 0) {
             rest /= kPrime[i];
             ++e[i];
@@ -148,6 +149,8 @@ inline bool mixedRadix(uint32_t n, MixedRadix* m) {
         for (; f[3] >= 1; --f[3]) push(f[0] >= 1 ? (--f[0], 14) : 7);
         for (; f[2] >= 1; --f[2]) push(f[0] >= 1 ? (--f[0], 10) : 5);
         for (; f[1] >= 1; --f[1]) push(f[0] >= 2 ? (f[0] -= 2, 12) : f[0] >= 1 ? (--f[0], 6) : 3);
+        for (int i = 0; i < e[4]; ++i) push(11);
+        for (int i = 0; i < e[5]; ++i) push(13);
         for (; f[0] >= 4; f[0] -= 4) push(16);
         if (f[0] >= 1) push(1 << f[0]);
         return r;

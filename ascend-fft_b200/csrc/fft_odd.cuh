@@ -1,5 +1,5 @@
-// Small odd-length DFTs in registers (3, 5, 7, 9) and Good-Thomas composites (6, 10, 12, 14,
-// 15), natural order in and out, forward sign
+// Small odd-length DFTs in registers (3, 5, 7, 9, 11, 13) and Good-Thomas composites (6, 10,
+// 12, 14, 15), natural order in and out, forward sign
 // exp(-2*pi*i*j*k/R) (INV flips it), and their DFT<R, INV> specialisations for the radix
 // passes.  Each pairs x[m] with x[R-m]: t = x[m] + x[R-m], d = x[m] - x[R-m], then
 //   X[k]   = x0 + sum_m cos(2 pi k m / R) t_m  -/+  i sum_m sin(2 pi k m / R) d_m
@@ -65,6 +65,91 @@ __device__ __forceinline__ void dft7(float2* x) {
     x[5] = csub(a2, b2);
     x[3] = cadd(a3, b3);
     x[4] = csub(a3, b3);
+}
+
+// Odd prime R = 11, 13 by the same symmetric pairs: (R-1)/2 cosine and sine sums per output pair.
+// cos / sin of 2 pi q / R for q = 1 .. (R-1)/2; larger q by symmetry (cos even, sin odd about R/2).
+__host__ __device__ constexpr float cos11(int q) {
+    switch (q) {
+        case 1: return 8.412535328311812055e-1f;
+        case 2: return 4.154150130018864351e-1f;
+        case 3: return -1.423148382732851436e-1f;
+        case 4: return -6.548607339452851006e-1f;
+        case 5: return -9.594929736144973687e-1f;
+        default: return 0.f;
+    }
+}
+__host__ __device__ constexpr float sin11(int q) {
+    switch (q) {
+        case 1: return 5.406408174555975554e-1f;
+        case 2: return 9.096319953545183301e-1f;
+        case 3: return 9.898214418809326842e-1f;
+        case 4: return 7.557495743542582689e-1f;
+        case 5: return 2.817325568414296710e-1f;
+        default: return 0.f;
+    }
+}
+__host__ __device__ constexpr float cos13(int q) {
+    switch (q) {
+        case 1: return 8.854560256532099105e-1f;
+        case 2: return 5.680647467311558119e-1f;
+        case 3: return 1.205366802553230476e-1f;
+        case 4: return -3.546048870425356214e-1f;
+        case 5: return -7.485107481711010813e-1f;
+        case 6: return -9.709418174260520118e-1f;
+        default: return 0.f;
+    }
+}
+__host__ __device__ constexpr float sin13(int q) {
+    switch (q) {
+        case 1: return 4.647231720437685620e-1f;
+        case 2: return 8.229838658936563522e-1f;
+        case 3: return 9.927088740980539727e-1f;
+        case 4: return 9.350162426854148334e-1f;
+        case 5: return 6.631226582407951931e-1f;
+        case 6: return 2.393156642875577667e-1f;
+        default: return 0.f;
+    }
+}
+template <int R>
+__host__ __device__ constexpr float prime_cos(int q) {
+    const int r = q <= R / 2 ? q : R - q;
+    return q == 0 ? 1.f : (R == 11 ? cos11(r) : cos13(r));
+}
+template <int R>
+__host__ __device__ constexpr float prime_sin(int q) {
+    const int r = q <= R / 2 ? q : R - q;
+    const float v = R == 11 ? sin11(r) : sin13(r);
+    return q <= R / 2 ? v : -v;
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_prime(float2* x) {
+    constexpr int H = (R - 1) / 2;
+    float2 t[H + 1], d[H + 1];
+#pragma unroll
+    for (int m = 1; m <= H; ++m) {
+        t[m] = cadd(x[m], x[R - m]);
+        d[m] = csub(x[m], x[R - m]);
+    }
+    const float2 x0 = x[0];
+    float2 sum = x0;
+#pragma unroll
+    for (int m = 1; m <= H; ++m) sum = cadd(sum, t[m]);
+#pragma unroll
+    for (int k = 1; k <= H; ++k) {
+        float2 a = x0, b = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int m = 1; m <= H; ++m) {
+            const float c = prime_cos<R>((k * m) % R), s = prime_sin<R>((k * m) % R);
+            a = make_float2(fmaf(c, t[m].x, a.x), fmaf(c, t[m].y, a.y));
+            b = make_float2(fmaf(s, d[m].x, b.x), fmaf(s, d[m].y, b.y));
+        }
+        b = mul_i(b, !INV);
+        x[k] = cadd(a, b);
+        x[R - k] = csub(a, b);
+    }
+    x[0] = sum;
 }
 
 // 9 = 3 x 3 Cooley-Tukey: j = 3 j1 + j2, k = k1 + 3 k2, inner twiddles W_9^(j2 k1).
@@ -137,6 +222,12 @@ template <bool INV> struct DFT<5, INV> {
 };
 template <bool INV> struct DFT<7, INV> {
     static __device__ __forceinline__ void run(float2* v) { dft7<INV>(v); }
+};
+template <bool INV> struct DFT<11, INV> {
+    static __device__ __forceinline__ void run(float2* v) { dft_prime<11, INV>(v); }
+};
+template <bool INV> struct DFT<13, INV> {
+    static __device__ __forceinline__ void run(float2* v) { dft_prime<13, INV>(v); }
 };
 template <bool INV> struct DFT<9, INV> {
     static __device__ __forceinline__ void run(float2* v) { dft9<INV>(v); }

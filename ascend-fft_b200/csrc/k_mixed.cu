@@ -1,4 +1,5 @@
-// Mixed-radix C2C for 7-smooth lengths (n = 2^a 3^b 5^c 7^d up to kMixedMaxN), one HBM pass.
+// Mixed-radix C2C for 13-smooth lengths (n = 2^a 3^b 5^c 7^d 11^e 13^f up to kMixedMaxN), one
+// HBM pass.
 // Stockham autosort: pass p of radix R over Ns = R_0 ... R_(p-1) takes butterfly j < n/R,
 // k = j mod Ns, inputs x[j + r n/R], twiddles W_(Ns R)^(k r) from the pass's slice of an
 // FP64-built table (entry (r-1) Ns + k: consecutive threads read consecutive entries), an
@@ -67,10 +68,16 @@ __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float
     }
 }
 
-template <bool INV, int KIND>
+// WIDE adds the prime radices 11 and 13 (their butterflies need more registers, so plans
+// without them run an instance compiled without those cases).
+template <bool INV, int KIND, bool WIDE>
 __device__ __forceinline__ void mixed_pass_r(int R, const float2* src, float2* dst, int n, int Ns, unsigned magic,
                                              const float2* twp, int t, int T, float scale, int pad0,
                                              unsigned magic0) {
+    if constexpr (WIDE) {
+        if (R == 13) return mixed_pass<13, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0);
+        if (R == 11) return mixed_pass<11, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0);
+    }
 #define BFLY_MP(RR) \
     case RR: mixed_pass<RR, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0); break
     switch (R) {
@@ -91,7 +98,7 @@ __device__ __forceinline__ void mixed_pass_r(int R, const float2* src, float2* d
 #undef BFLY_MP
 }
 
-template <bool INV>
+template <bool INV, bool WIDE>
 __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in, float2* __restrict__ out,
                                                   const float2* __restrict__ tw, MixedArgs a, uint64_t batch, int T,
                                                   int rows, int len, float scale) {
@@ -115,12 +122,12 @@ __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in,
         const int p0 = a.pad0;
         const unsigned m0 = a.magic0;
         if (ok) {
-            if (first && last) mixed_pass_r<INV, 3>(R, src, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (first) mixed_pass_r<INV, 1>(R, src, d, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (p == 1 && last) mixed_pass_r<INV, 6>(R, s, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (p == 1) mixed_pass_r<INV, 4>(R, s, d, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (last) mixed_pass_r<INV, 2>(R, s, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else mixed_pass_r<INV, 0>(R, s, d, n, Ns, mg, twp, t, T, scale, p0, m0);
+            if (first && last) mixed_pass_r<INV, 3, WIDE>(R, src, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (first) mixed_pass_r<INV, 1, WIDE>(R, src, d, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (p == 1 && last) mixed_pass_r<INV, 6, WIDE>(R, s, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (p == 1) mixed_pass_r<INV, 4, WIDE>(R, s, d, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (last) mixed_pass_r<INV, 2, WIDE>(R, s, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else mixed_pass_r<INV, 0, WIDE>(R, s, d, n, Ns, mg, twp, t, T, scale, p0, m0);
         }
         if (!last) __syncthreads();
     }
@@ -195,7 +202,10 @@ int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batc
     }
     args.magic0 = args.pad0 ? (unsigned)((0x100000000ull + args.pad0 - 1) / (unsigned long long)args.pad0) : 0u;
     const int smem = rows * 2 * len * 8;
-    auto* fn = inverse ? dev::k_mixed<true> : dev::k_mixed<false>;
+    bool wide = false;
+    for (int p = 0; p < plan.passes; ++p) wide = wide || plan.radix[p] == 11 || plan.radix[p] == 13;
+    auto* fn = inverse ? (wide ? dev::k_mixed<true, true> : dev::k_mixed<true, false>)
+                       : (wide ? dev::k_mixed<false, true> : dev::k_mixed<false, false>);
     // opted in once per device at kMaxSmem (the largest row pair: n = kMixedMaxN, one row per CTA)
     if (smem > kMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMaxSmem)) return e;

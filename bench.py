@@ -394,7 +394,7 @@ def extra_measurements(dev, stream):
     # ---- non-power-of-two C2C, batch * n ~ 2^25: prime-factor kernel (n = A * 2^k) and
     # Bluestein (other lengths), one kernel each
     out["c2c_any_length"] = {}
-    for n in (1536, 1920, 6144, 360, 1000, 3000, 6561, 12000, 1001, 8191):
+    for n in (1536, 1920, 6144, 360, 1000, 3000, 6561, 12000, 1001, 1003, 8191):
         b = (1 << 25) // n
         g = torch.Generator(device=dev).manual_seed(n)
         x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
@@ -404,7 +404,7 @@ def extra_measurements(dev, stream):
         gbs = 16 * n * b / ms / 1e6
         pfa = any(n % a == 0 and (n // a) & (n // a - 1) == 0 and n // a >= 16 for a in (3, 5, 9, 15))
         m = n
-        for p in (2, 3, 5, 7):
+        for p in (2, 3, 5, 7, 11, 13):
             while m % p == 0:
                 m //= p
         kernel = ("prime-factor" if pfa else "mixed-radix" if m == 1 and n <= 12288

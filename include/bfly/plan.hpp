@@ -205,7 +205,7 @@ public:
     //   direction -1 forward, +1 inverse; scale multiplies the output.
     //   n in [32, 16384] single pass, [8192, 65536] four-step (workspace grown on demand);
     //   n = A * 2^k (A in {3, 5, 9, 15}, 2^k >= 16, n <= 12288) by the prime-factor mapping in
-    //   one kernel; other n = 2^a 3^b 5^c 7^d <= 12288 (2..16 included) by mixed-radix Stockham
+    //   one kernel; other n = 2^a 3^b 5^c 7^d 11^e 13^f <= 12288 (2..16 included) by mixed-radix Stockham
     //   passes in one kernel; any other n in [2, 8192] by Bluestein's algorithm in one kernel
     //   (the first call for a length builds its tables).
     int execC2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, int direction,

@@ -128,7 +128,7 @@ int bfly_plan_run_c2c_long(bfly_plan* plan, const float* in, float* out, uint32_
  * its twiddle tables (and the four-step workspace) and synchronises the context stream once;
  * make it before any stream capture. */
 /* C2C, power-of-two n in [32, 65536]; n = A*2^k (A in {3, 5, 9, 15}, 2^k >= 16, n <= 12288) by
- * the prime-factor mapping in one kernel; other n = 2^a 3^b 5^c 7^d <= 12288 (2..16 included) by
+ * the prime-factor mapping in one kernel; other n = 2^a 3^b 5^c 7^d 11^e 13^f <= 12288 (2..16 included) by
  * mixed-radix Stockham passes in one kernel; any other n in [2, 8192] by Bluestein's algorithm
  * in one kernel (the reference supports powers of two only, docs/reference/support.md:14);
  * direction -1 forward / +1 inverse; output multiplied by scale. */

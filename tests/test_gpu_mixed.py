@@ -1,9 +1,9 @@
-"""Mixed-radix C2C (Stockham passes of radix 16/8/4/2/7/5/3 through shared memory) against FP64
-numpy, for every 7-smooth length the kernel serves.
+"""Mixed-radix C2C (Stockham passes of radix 2..16, odd primes up to 13 and composites, through
+shared memory) against FP64 numpy, for every length the kernel serves.
 
 The reference supports power-of-two lengths only (docs/testing.md:16-17 lists radix-3/5/7 as
-missing).  The kernel takes n = 2^a 3^b 5^c 7^d up to 12288 that is neither a power of two >= 32
-(Stockham team kernels) nor A*2^k with A in {3, 5, 9, 15} (prime-factor kernel).  Tolerance:
+missing).  The kernel takes n = 2^a 3^b 5^c 7^d 11^e 13^f up to 12288 that is neither a power of
+two >= 32 (Stockham team kernels) nor A*2^k with A in {3, 5, 9, 15} (prime-factor kernel).  Tolerance:
 rel L2 <= 1e-6 per row against FP64, the single-pass C2C gate, plus the reference's
 maxRelScaled <= 1e-4."""
 import numpy as np
@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _smooth(n):
-    for p in (2, 3, 5, 7):
+    for p in (2, 3, 5, 7, 11, 13):
         while n % p == 0:
             n //= p
     return n == 1
@@ -42,8 +42,8 @@ def _check(plan, cuda, n, batch, direction, seed):
 
 
 def test_every_mixed_length(plan, cuda):
-    """All 324 lengths, forward and inverse, 3 rows each."""
-    assert len(MIXED) > 300
+    """All 760 lengths, forward and inverse, 3 rows each."""
+    assert len(MIXED) > 700
     worst = (0.0, None)
     for n in MIXED:
         for direction in (-1, 1):
@@ -53,7 +53,8 @@ def test_every_mixed_length(plan, cuda):
     print("worst rel L2", worst)
 
 
-@pytest.mark.parametrize("n", [6, 60, 100, 360, 1000, 2401, 3000, 5000, 6561, 10935, 12000, 12250])
+@pytest.mark.parametrize("n", [6, 60, 100, 360, 1000, 2401, 3000, 5000, 6561, 10935, 12000, 12250, 11, 143, 1001,
+                               4095, 1331, 2197, 9152])
 @pytest.mark.parametrize("direction", [-1, 1])
 def test_mixed_large_batches(plan, cuda, n, direction):
     """Many rows per launch, batch not a multiple of the rows per CTA."""
@@ -65,7 +66,7 @@ def test_mixed_large_batches(plan, cuda, n, direction):
 def test_mixed_known_answers_and_in_place(plan, cuda):
     """Impulse at p -> exp(-2 pi i p k / n); constant -> n at bin 0; in place equals out of place."""
     import torch
-    for n in (7, 49, 1000, 2401, 11025):
+    for n in (7, 13, 49, 1000, 1001, 2401, 11025):
         pos = [0, 1, 3, n // 2, n - 1]
         x = torch.zeros(len(pos) + 1, n, dtype=torch.complex64, device=cuda)
         for r, p in enumerate(pos):
