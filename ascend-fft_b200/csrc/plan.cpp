@@ -1099,19 +1099,37 @@ int Plan::runMany(const HostRequest* reqs, size_t count) {
         groupBytes = 0;
         return 0;
     };
-    size_t off = 0;
-    for (size_t i = 0; i < count; ++i) {
+    // Issue order: every other request by size goes first (smallest first), the rest last
+    // (largest first), so the largest requests stream in the middle and both ends of the
+    // pipeline are short; near the end pieces shrink to half of what is left (at least
+    // 512 KB), so the final download trailing the last upload is short.  Measured over the
+    // 49-point grid with pinned buffers: +2 % against request order and fixed 16 MB pieces;
+    // smaller fixed pieces lose (each copy costs microseconds of its own).
+    std::vector<size_t> offs(count), bySize(count), order;
+    size_t remaining = 0;
+    for (size_t i = 0, off = 0; i < count; ++i) {
+        offs[i] = off;
+        off += up((size_t)reqs[i].n * reqs[i].batch * 8);
+        remaining += (size_t)reqs[i].n * reqs[i].batch * 8;
+        bySize[i] = i;
+    }
+    auto bytesOf = [&](size_t i) { return (size_t)reqs[i].n * reqs[i].batch; };
+    std::stable_sort(bySize.begin(), bySize.end(), [&](size_t a, size_t b) { return bytesOf(a) < bytesOf(b); });
+    for (size_t k = 0; k < count; k += 2) order.push_back(bySize[k]);
+    for (size_t k = count - 1 - (count % 2 == 0 ? 0 : 1); k < count; k -= 2) order.push_back(bySize[k]);
+    for (const size_t i : order) {
         const HostRequest& r = reqs[i];
         const size_t rowBytes = (size_t)r.n * 8;
-        const uint32_t chunk = (uint32_t)std::max<size_t>(1, kChunkBytes / rowBytes);
-        for (uint32_t r0 = 0; r0 < r.batch; r0 += chunk) {
-            const uint32_t rows = std::min(chunk, r.batch - r0);
-            group.push_back({&r, off + (size_t)r0 * rowBytes, r0, rows});
+        for (uint32_t r0 = 0; r0 < r.batch;) {
+            const size_t want = std::min<size_t>(kChunkBytes, std::max<size_t>(512u << 10, remaining / 2));
+            const uint32_t rows = (uint32_t)std::min<size_t>(r.batch - r0, std::max<size_t>(1, want / rowBytes));
+            group.push_back({&r, offs[i] + (size_t)r0 * rowBytes, r0, rows});
             groupBytes += (size_t)rows * rowBytes;
+            remaining -= (size_t)rows * rowBytes;
+            r0 += rows;
             if (groupBytes >= kGroupBytes)
                 if (int rc = flush()) return rc;
         }
-        off += up((size_t)r.n * r.batch * 8);
     }
     if (int rc = flush()) return rc;
     if (backend::streamSync(sIn) || backend::streamSync(stream_)) return -6;
