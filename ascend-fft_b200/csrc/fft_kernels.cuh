@@ -193,7 +193,7 @@ k_cols(const float2* __restrict__ in, float2* __restrict__ out, const float2* __
 // Pass A: C consecutive columns per CTA, column index fastest across threads so each global
 // access is C consecutive complex values (C*8 bytes).
 template <int N1, int E, int C, bool INV>
-__global__ void __launch_bounds__((N1 / E) * C)
+__global__ void __launch_bounds__((N1 / E) * C, 3)
 k_long_a(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
          const float2* __restrict__ tlo, const float2* __restrict__ thi, uint64_t batch, int logN2) {
     constexpr int T = N1 / E;
