@@ -13,7 +13,8 @@ hand-written adjoints behind torch.autograd.Function:
                             window and one-sided transform in one kernel
     istft(X, n_fft, ...)    complex64 [..., n_fft/2+1, frames] -> float32 [..., L], torch.istft's
                             arguments; C2R of every frame, then a windowed overlap-add kernel
-    rfft(x)                 float32 [..., n] -> complex64 [..., n/2+1], n in 64..8192
+    rfft(x)                 float32 [..., n] -> complex64 [..., n/2+1], n in 64..8192 a power of
+                            two, or even with n/2 13-smooth (up to 24576)
     irfft(X, n)             complex64 [..., n/2+1] -> float32 [..., n]
 
 `norm` follows torch.fft ("backward", "ortho", "forward").  Adjoints:

@@ -166,6 +166,16 @@ inline bool mixedRadix(uint32_t n, MixedRadix* m) {
 int buildMixedTwiddles(void* tw, const MixedRadix& plan, void* stream);   // FP64 on the device
 int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
                 const void* tw, void* stream);
+// Real transforms of even n = 2M with the M-point passes `half` (M 13-smooth): R2C / C2R with
+// the layouts, split and per-bin weights of launchR2C / launchC2R, and the STFT of launchStft;
+// twr = W_n^k, k <= M (linear table of M + 1 entries).
+int launchR2CMixed(const void* in, void* out, const MixedRadix& half, uint64_t batch, const void* tw, const void* twr,
+                   float sEdge, float sInt, void* stream);
+int launchC2RMixed(const void* in, void* out, const MixedRadix& half, uint64_t batch, const void* tw, const void* twr,
+                   float sEdge, float sInt, float outScale, void* stream);
+int launchStftMixed(const void* sig, void* out, const MixedRadix& half, uint64_t signals, uint32_t framesPerSignal,
+                    uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,
+                    const void* tw, const void* twr, void* stream);
 
 // STFT: `signals` real signals of sigLen samples (signal s at s*sigStride floats), frames of n
 // samples every `hop` (centred with reflect padding when `center`), times `window` (n floats,

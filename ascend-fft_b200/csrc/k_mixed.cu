@@ -41,20 +41,25 @@ __device__ __forceinline__ int mixed_at(int i, int pad0, unsigned magic0) {
 }
 
 // KIND bit 0: source is the row in HBM (pass 0, which writes the pass-0 buffer); bit 1:
-// destination is the row in HBM (scaled); bit 2: source is the pass-0 buffer (pass 1).
-// Pass 0 (Ns = 1) has no twiddles.
+// destination is the row in HBM (scaled); bit 2: source is the pass-0 buffer (pass 1); bit 3:
+// source is a row staged unpadded in shared memory (pass 0); bit 4: destination is shared
+// memory, unpadded, in natural order (the last pass, for an epilogue).  Pass 0 (Ns = 1) has no
+// twiddles.
 template <int R, bool INV, int KIND>
 __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float2* __restrict__ dst, int n, int Ns,
                                            unsigned magic, const float2* __restrict__ twp, int t, int T,
                                            float scale, int pad0, unsigned magic0) {
+    constexpr bool PASS0 = (KIND & 9) != 0;
     const int nb = n / R;
     for (int j = t; j < nb; j += T) {
-        const int k = (KIND & 1) ? 0 : j - Ns * (int)__umulhi((unsigned)j, magic);
+        const int k = PASS0 ? 0 : j - Ns * (int)__umulhi((unsigned)j, magic);
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r)
-            v[r] = (KIND & 1) ? ld_stream(src + j + r * nb) : src[mixed_at<(KIND & 4) != 0>(j + r * nb, pad0, magic0)];
-        if (!(KIND & 1)) {
+            v[r] = (KIND & 1)   ? ld_stream(src + j + r * nb)
+                   : (KIND & 8) ? src[j + r * nb]
+                                : src[mixed_at<(KIND & 4) != 0>(j + r * nb, pad0, magic0)];
+        if (!PASS0) {
 #pragma unroll
             for (int r = 1; r < R; ++r) v[r] = cmul<INV>(v[r], __ldg(twp + (r - 1) * Ns + k));
         }
@@ -63,7 +68,8 @@ __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (KIND & 2) st_stream(dst + base + r * Ns, cscale(v[r], scale));
-            else dst[mixed_at<(KIND & 1) != 0>(base + r * Ns, pad0, magic0)] = v[r];
+            else if (KIND & 16) dst[base + r * Ns] = v[r];
+            else dst[mixed_at<PASS0>(base + r * Ns, pad0, magic0)] = v[r];
         }
     }
 }
@@ -98,6 +104,42 @@ __device__ __forceinline__ void mixed_pass_r(int R, const float2* src, float2* d
 #undef BFLY_MP
 }
 
+// The passes of one row.  Pass 0 reads the row from HBM (SRC_HBM) or unpadded from buf1 (a
+// stage written before the call); the last pass writes the row to HBM times `scale` (DST_HBM)
+// or unpadded, natural order, into the buffer returned (buf0 or buf1).  All threads of the CTA
+// call it (rows whose `ok` is false skip the work, not the barriers).
+template <bool INV, bool WIDE, bool SRC_HBM, bool DST_HBM>
+__device__ __forceinline__ float2* mixed_row(const MixedArgs& a, const float2* src, float2* dst, float2* buf0,
+                                             float2* buf1, const float2* __restrict__ tw, bool ok, int t, int T,
+                                             float scale) {
+    constexpr int K0 = SRC_HBM ? 1 : 8;       // pass-0 source
+    constexpr int KL = DST_HBM ? 2 : 16;      // last-pass destination
+    const int n = a.n;
+    float2* fin = buf0;
+    for (int p = 0; p < a.passes; ++p) {
+        const int R = a.radix[p], Ns = a.ns[p];
+        const unsigned mg = a.magic[p];
+        const float2* twp = tw + a.twoff[p];
+        const bool first = p == 0, last = p == a.passes - 1;
+        const float2* sb = (p & 1) ? buf0 : buf1;   // written by pass p - 1 (pass 0: the stage)
+        float2* db = (p & 1) ? buf1 : buf0;
+        float2* dl = DST_HBM ? dst : db;
+        const int p0 = a.pad0;
+        const unsigned m0 = a.magic0;
+        if (ok) {
+            if (first && last) mixed_pass_r<INV, K0 | KL, WIDE>(R, SRC_HBM ? src : sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (first) mixed_pass_r<INV, K0, WIDE>(R, SRC_HBM ? src : sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (p == 1 && last) mixed_pass_r<INV, 4 | KL, WIDE>(R, sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (p == 1) mixed_pass_r<INV, 4, WIDE>(R, sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (last) mixed_pass_r<INV, KL, WIDE>(R, sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else mixed_pass_r<INV, 0, WIDE>(R, sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
+        }
+        if (last) fin = db;
+        if (!last) __syncthreads();
+    }
+    return fin;
+}
+
 template <bool INV, bool WIDE>
 __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in, float2* __restrict__ out,
                                                   const float2* __restrict__ tw, MixedArgs a, uint64_t batch, int T,
@@ -107,29 +149,110 @@ __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in,
     const int t = threadIdx.x - rl * T;
     const uint64_t row = (uint64_t)blockIdx.x * rows + rl;
     const bool ok = rl < rows && row < batch;
-    const int n = a.n;
-    const float2* src = in + row * n;
-    float2* dst = out + row * n;
+    float2* buf0 = smem + (size_t)(rl < rows ? rl : 0) * 2 * len;
+    mixed_row<INV, WIDE, true, true>(a, in + row * a.n, out + row * a.n, buf0, buf0 + len, tw, ok, t, T, scale);
+}
+
+// Real transforms of even length N = 2M on the mixed-radix passes of the M-point complex row
+// (M 13-smooth).  twr[k] = W_N^k, k <= M.
+// R2C (numpy.fft.rfft): z[m] = x[2m] + i x[2m+1] read as complex, Z = FFT_M(z) left unpadded in
+// shared memory, then per bin k <= M: a = Z[k mod M], b = conj(Z[(M-k) mod M]),
+// X[k] = (a+b)/2 + W_N^k (a-b)/(2i), times s_edge at bins 0 and M and s_int elsewhere.
+template <bool WIDE>
+__global__ void __launch_bounds__(512, 2) k_r2c_mixed(const float2* __restrict__ in, float2* __restrict__ out,
+                                                      const float2* __restrict__ tw, const float2* __restrict__ twr,
+                                                      MixedArgs a, uint64_t batch, int T, int rows, int len,
+                                                      float s_edge, float s_int) {
+    extern __shared__ float2 smem[];
+    const int rl = threadIdx.x / T;
+    const int t = threadIdx.x - rl * T;
+    const uint64_t row = (uint64_t)blockIdx.x * rows + rl;
+    const bool ok = rl < rows && row < batch;
+    const int M = a.n;
+    float2* buf0 = smem + (size_t)(rl < rows ? rl : 0) * 2 * len;
+    const float2* Z = mixed_row<false, WIDE, true, false>(a, in + row * M, nullptr, buf0, buf0 + len, tw, ok, t, T,
+                                                           1.f);
+    __syncthreads();
+    if (!ok) return;
+    float2* dst = out + row * (uint64_t)(M + 1);
+    for (int k = t; k <= M; k += T) {
+        const float2 za = Z[k < M ? k : 0];
+        const float2 zb = Z[k > 0 ? M - k : 0];
+        const float2 e = make_float2(0.5f * (za.x + zb.x), 0.5f * (za.y - zb.y));
+        const float2 o = make_float2(0.5f * (za.y + zb.y), 0.5f * (zb.x - za.x));
+        const float2 X = cadd(e, cmul<false>(o, __ldg(twr + k)));
+        st_stream(dst + k, cscale(X, (k == 0 || k == M) ? s_edge : s_int));
+    }
+}
+
+// C2R (numpy.fft.irfft when out_scale = 1/N, as k_c2r): the un-split spectrum
+// Z[k] = (Xk + conj Xm) + i (Xk - conj Xm) W_N^-k (Xm = X[M-k], X[M] for k = 0; imaginary parts of
+// bins 0 and M ignored; s_edge / s_int per bin; out_scale) is staged unpadded in shared memory,
+// then z = IFFT_M(Z) goes to HBM as x[2m] = Re z[m], x[2m+1] = Im z[m].
+template <bool WIDE>
+__global__ void __launch_bounds__(512, 2) k_c2r_mixed(const float2* __restrict__ in, float2* __restrict__ out,
+                                                      const float2* __restrict__ tw, const float2* __restrict__ twr,
+                                                      MixedArgs a, uint64_t batch, int T, int rows, int len,
+                                                      float s_edge, float s_int, float out_scale) {
+    extern __shared__ float2 smem[];
+    const int rl = threadIdx.x / T;
+    const int t = threadIdx.x - rl * T;
+    const uint64_t row = (uint64_t)blockIdx.x * rows + rl;
+    const bool ok = rl < rows && row < batch;
+    const int M = a.n;
     float2* buf0 = smem + (size_t)(rl < rows ? rl : 0) * 2 * len;
     float2* buf1 = buf0 + len;
-    for (int p = 0; p < a.passes; ++p) {
-        const int R = a.radix[p], Ns = a.ns[p];
-        const unsigned mg = a.magic[p];
-        const float2* twp = tw + a.twoff[p];
-        const bool first = p == 0, last = p == a.passes - 1;
-        const float2* s = (p & 1) ? buf0 : buf1;   // written by pass p - 1
-        float2* d = (p & 1) ? buf1 : buf0;
-        const int p0 = a.pad0;
-        const unsigned m0 = a.magic0;
-        if (ok) {
-            if (first && last) mixed_pass_r<INV, 3, WIDE>(R, src, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (first) mixed_pass_r<INV, 1, WIDE>(R, src, d, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (p == 1 && last) mixed_pass_r<INV, 6, WIDE>(R, s, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (p == 1) mixed_pass_r<INV, 4, WIDE>(R, s, d, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (last) mixed_pass_r<INV, 2, WIDE>(R, s, dst, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else mixed_pass_r<INV, 0, WIDE>(R, s, d, n, Ns, mg, twp, t, T, scale, p0, m0);
+    const float2* src = in + row * (uint64_t)(M + 1);
+    if (ok)
+        for (int k = t; k < M; k += T)
+            buf1[k] = c2r_split(ld_stream(src + k), ld_stream(src + (k == 0 ? M : M - k)), k, __ldg(twr + k), s_edge,
+                                s_int, out_scale);
+    __syncthreads();
+    mixed_row<true, WIDE, false, true>(a, nullptr, out + row * M, buf0, buf1, tw, ok, t, T, 1.f);
+}
+
+// STFT: frame f of signal s, y[j] = w[j] x_s[f hop + j - (center ? N/2 : 0)] (reflect padding,
+// as k_stft), packed as z[m] = y[2m] + i y[2m+1] and staged unpadded; then the R2C of k_r2c_mixed.
+template <bool WIDE>
+__global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__ sig, float2* __restrict__ out,
+                                                       const float2* __restrict__ tw, const float2* __restrict__ twr,
+                                                       const float* __restrict__ window, MixedArgs a, uint64_t frames,
+                                                       uint32_t framesPerSignal, int64_t sigLen, uint64_t sigStride,
+                                                       uint32_t hop, int center, int T, int rows, int len) {
+    extern __shared__ float2 smem[];
+    const int rl = threadIdx.x / T;
+    const int t = threadIdx.x - rl * T;
+    const uint64_t row = (uint64_t)blockIdx.x * rows + rl;
+    const bool ok = rl < rows && row < frames;
+    const int M = a.n;
+    float2* buf0 = smem + (size_t)(rl < rows ? rl : 0) * 2 * len;
+    float2* buf1 = buf0 + len;
+    if (ok) {
+        const uint64_t s = row / framesPerSignal, f = row % framesPerSignal;
+        const float* x = sig + s * sigStride;
+        const int64_t start = (int64_t)f * hop - (center ? M : 0);
+        auto sample = [&](int64_t i) {
+            i = i < 0 ? -i : i;
+            i = i >= sigLen ? 2 * (sigLen - 1) - i : i;
+            return __ldg(x + i);
+        };
+        for (int m = t; m < M; m += T) {
+            float2 z = make_float2(sample(start + 2 * m), sample(start + 2 * m + 1));
+            if (window) z = make_float2(z.x * __ldg(window + 2 * m), z.y * __ldg(window + 2 * m + 1));
+            buf1[m] = z;
         }
-        if (!last) __syncthreads();
+    }
+    __syncthreads();
+    const float2* Z = mixed_row<false, WIDE, false, false>(a, nullptr, nullptr, buf0, buf1, tw, ok, t, T, 1.f);
+    __syncthreads();
+    if (!ok) return;
+    float2* dst = out + row * (uint64_t)(M + 1);
+    for (int k = t; k <= M; k += T) {
+        const float2 za = Z[k < M ? k : 0];
+        const float2 zb = Z[k > 0 ? M - k : 0];
+        const float2 e = make_float2(0.5f * (za.x + zb.x), 0.5f * (za.y - zb.y));
+        const float2 o = make_float2(0.5f * (za.y + zb.y), 0.5f * (zb.x - za.x));
+        st_stream(dst + k, cadd(e, cmul<false>(o, __ldg(twr + k))));
     }
 }
 
@@ -177,43 +300,109 @@ int buildMixedTwiddles(void* tw, const MixedRadix& plan, void* stream) {
     return (int)cudaGetLastError();
 }
 
-int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
-                const void* tw, void* stream) {
-    if (!mixedValid(plan)) return (int)cudaErrorInvalidValue;
-    // one butterfly of the largest radix per thread and pass (more of the smaller radices)
+namespace {
+// Launch shape of the mixed-radix kernels for one M-point complex row (k_mixed and the real
+// transforms built on it): threads per row, rows per CTA, buffer length and the pass-0 pad.
+struct MixedShape {
+    dev::MixedArgs args;
+    int T = 0, rows = 0, len = 0, smem = 0;
+    bool wide = false;
+};
+constexpr int kMixedMaxSmem = 2 * (dev::spad((int)kMixedMaxN - 1) + 1) * 8;
+static_assert(kMixedMaxSmem <= 227 * 1024, "two rows of the longest length fit in shared memory");
+
+MixedShape mixedShape(const MixedRadix& plan) {
+    MixedShape m;
+    m.args = mixedArgs(plan);
+    // one butterfly of the largest radix per thread and pass (more of the smaller radices);
+    // measured on B200 over n = 12..12000: ceil(n / R_max) threads per row with ~200-300
+    // threads per CTA beat n/8 threads per row, larger CTAs, and an 80-register budget
     int rmax = 2;
-    for (int p = 0; p < plan.passes; ++p) rmax = std::max(rmax, plan.radix[p]);
-    // measured on B200 over n = 12..12000: ceil(n / R_max) threads per row with ~200-300 threads
-    // per CTA beat n/8 threads per row, larger CTAs, and an 80-register budget
-    const int T = std::min(512, (plan.n + rmax - 1) / rmax);
-    const int rows = std::max(1, 224 / T);
-    constexpr int kMaxSmem = 2 * (dev::spad((int)kMixedMaxN - 1) + 1) * 8;
-    static_assert(kMaxSmem <= 227 * 1024, "two rows of the longest length fit in shared memory");
-    dev::MixedArgs args = mixedArgs(plan);
+    for (int p = 0; p < plan.passes; ++p) {
+        rmax = std::max(rmax, plan.radix[p]);
+        m.wide = m.wide || plan.radix[p] == 11 || plan.radix[p] == 13;
+    }
+    m.T = std::min(512, (plan.n + rmax - 1) / rmax);
+    m.rows = std::max(1, 224 / m.T);
     // pass 0 stores at stride R_0: pad its buffer every R_0 slots when R_0 is even (odd strides
     // are conflict-free already), unless that no longer fits; pad 16 is spad's layout
     const int r0 = plan.radix[0];
-    int len = dev::spad(plan.n - 1) + 1;
-    args.pad0 = (r0 % 2 == 0 && plan.passes > 1) ? r0 : 0;
-    if (args.pad0) {
-        const int len0 = std::max(len, plan.n + (plan.n - 1) / args.pad0 + 1);
-        if (rows * 2 * len0 * 8 <= kMaxSmem) len = len0;
-        else args.pad0 = 16;
+    m.len = dev::spad(plan.n - 1) + 1;
+    m.args.pad0 = (r0 % 2 == 0 && plan.passes > 1) ? r0 : 0;
+    if (m.args.pad0) {
+        const int len0 = std::max(m.len, plan.n + (plan.n - 1) / m.args.pad0 + 1);
+        if (m.rows * 2 * len0 * 8 <= kMixedMaxSmem) m.len = len0;
+        else m.args.pad0 = 16;
     }
-    args.magic0 = args.pad0 ? (unsigned)((0x100000000ull + args.pad0 - 1) / (unsigned long long)args.pad0) : 0u;
-    const int smem = rows * 2 * len * 8;
-    bool wide = false;
-    for (int p = 0; p < plan.passes; ++p) wide = wide || plan.radix[p] == 11 || plan.radix[p] == 13;
-    auto* fn = inverse ? (wide ? dev::k_mixed<true, true> : dev::k_mixed<true, false>)
-                       : (wide ? dev::k_mixed<false, true> : dev::k_mixed<false, false>);
-    // opted in once per device at kMaxSmem (the largest row pair: n = kMixedMaxN, one row per CTA)
-    if (smem > kMaxSmem) return (int)cudaErrorInvalidValue;
-    if (int e = optInSharedMemory((const void*)fn, kMaxSmem)) return e;
-    const uint64_t grid = (batch + rows - 1) / rows;
-    if (grid > 0x7fffffffull) return (int)cudaErrorInvalidValue;
-    fn<<<(unsigned)grid, T * rows, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw), args, batch, T,
-        rows, len, scale);
+    m.args.magic0 =
+        m.args.pad0 ? (unsigned)((0x100000000ull + m.args.pad0 - 1) / (unsigned long long)m.args.pad0) : 0u;
+    m.smem = m.rows * 2 * m.len * 8;
+    return m;
+}
+}  // namespace
+
+int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batch, bool inverse, float scale,
+                const void* tw, void* stream) {
+    if (!mixedValid(plan)) return (int)cudaErrorInvalidValue;
+    const MixedShape m = mixedShape(plan);
+    auto* fn = inverse ? (m.wide ? dev::k_mixed<true, true> : dev::k_mixed<true, false>)
+                       : (m.wide ? dev::k_mixed<false, true> : dev::k_mixed<false, false>);
+    // opted in once per device at kMixedMaxSmem (the largest row pair: n = kMixedMaxN, one row per CTA)
+    if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
+    if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
+    const uint64_t groups = (batch + m.rows - 1) / m.rows;
+    if (groups > 0x7fffffffull) return (int)cudaErrorInvalidValue;
+    fn<<<(unsigned)groups, m.T * m.rows, m.smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw), m.args, batch, m.T,
+        m.rows, m.len, scale);
+    return (int)cudaGetLastError();
+}
+
+int launchR2CMixed(const void* in, void* out, const MixedRadix& half, uint64_t batch, const void* tw, const void* twr,
+                   float sEdge, float sInt, void* stream) {
+    if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
+    const MixedShape m = mixedShape(half);
+    auto* fn = m.wide ? dev::k_r2c_mixed<true> : dev::k_r2c_mixed<false>;
+    if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
+    if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
+    const uint64_t groups = (batch + m.rows - 1) / m.rows;
+    if (groups > 0x7fffffffull) return (int)cudaErrorInvalidValue;
+    fn<<<(unsigned)groups, m.T * m.rows, m.smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw),
+        static_cast<const float2*>(twr), m.args, batch, m.T, m.rows, m.len, sEdge, sInt);
+    return (int)cudaGetLastError();
+}
+
+int launchC2RMixed(const void* in, void* out, const MixedRadix& half, uint64_t batch, const void* tw, const void* twr,
+                   float sEdge, float sInt, float outScale, void* stream) {
+    if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
+    const MixedShape m = mixedShape(half);
+    auto* fn = m.wide ? dev::k_c2r_mixed<true> : dev::k_c2r_mixed<false>;
+    if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
+    if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
+    const uint64_t groups = (batch + m.rows - 1) / m.rows;
+    if (groups > 0x7fffffffull) return (int)cudaErrorInvalidValue;
+    fn<<<(unsigned)groups, m.T * m.rows, m.smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw),
+        static_cast<const float2*>(twr), m.args, batch, m.T, m.rows, m.len, sEdge, sInt, outScale);
+    return (int)cudaGetLastError();
+}
+
+int launchStftMixed(const void* sig, void* out, const MixedRadix& half, uint64_t signals, uint32_t framesPerSignal,
+                    uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,
+                    const void* tw, const void* twr, void* stream) {
+    if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
+    const MixedShape m = mixedShape(half);
+    auto* fn = m.wide ? dev::k_stft_mixed<true> : dev::k_stft_mixed<false>;
+    if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
+    if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
+    const uint64_t frames = signals * framesPerSignal;
+    const uint64_t groups = (frames + m.rows - 1) / m.rows;
+    if (groups > 0x7fffffffull) return (int)cudaErrorInvalidValue;
+    fn<<<(unsigned)groups, m.T * m.rows, m.smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<const float*>(sig), static_cast<float2*>(out), static_cast<const float2*>(tw),
+        static_cast<const float2*>(twr), static_cast<const float*>(window), m.args, frames, framesPerSignal,
+        (int64_t)sigLen, sigStride, hop, center ? 1 : 0, m.T, m.rows, m.len);
     return (int)cudaGetLastError();
 }
 

@@ -432,13 +432,17 @@ static int ensureBuf(void** p, size_t* cap, size_t bytes) {
     return 0;
 }
 
+// Real transforms of even n whose half length runs the mixed-radix kernel.
+static bool realMixed(uint32_t n) { return n >= 4 && n % 2 == 0 && backend::mixedRadix(n / 2, nullptr); }
+
 bool Plan::validShape(uint32_t n, uint32_t batch, int kind) const {
     if (!impl_ || batch == 0) return false;
     // lengths outside the power-of-two kernels (non-powers of two, and 2..16) only through the
-    // device-pointer C2C entry (prime-factor kernel for A*2^k, mixed radix for other 7-smooth
-    // lengths, else Bluestein)
+    // device-pointer entries: C2C by the prime-factor kernel for A*2^k, mixed radix for other
+    // 13-smooth lengths, else Bluestein; R2C / C2R of even n with n/2 13-smooth by mixed radix
     if (!pow2(n) || (kind == kExecC2C && n < kMinN)) {
         uint32_t a = 0, b = 0;
+        if (kind == kExecR2C || kind == kExecC2R) return realMixed(n);
         return kind == kExecC2C &&
                (backend::bluesteinM(n) != 0 || backend::pfaSplit(n, &a, &b) || backend::mixedRadix(n, nullptr));
     }
@@ -752,11 +756,20 @@ int Plan::execC2CAxis(const void* dIn, void* dOut, uint32_t n, uint64_t outer, u
 
 int Plan::execStft(const void* dSig, void* dOut, uint32_t n, uint64_t signals, uint64_t sigLen,
                    uint32_t hop, bool center, const void* dWindow, uint64_t* framesOut, void* stream) {
-    if (!impl_ || !dSig || !dOut || signals == 0 || hop == 0 || !backend::hasStft(n)) return -8;
+    const bool mixedN = !pow2(n) && realMixed(n);
+    if (!impl_ || !dSig || !dOut || signals == 0 || hop == 0 || !(backend::hasStft(n) || mixedN)) return -8;
     if (center ? sigLen <= n / 2 : sigLen < n) return -8;
     const uint64_t frames = center ? 1 + sigLen / hop : 1 + (sigLen - n) / hop;
     if (frames > 0xFFFFFFFFull || signals > (~0ull) / frames) return -8;
     if (framesOut) *framesOut = frames;
+    if (mixedN) {
+        if (prepareMixed(n / 2) || prepareReal(n)) return -2;
+        const auto& m = impl_->mixed[n / 2];
+        if (backend::launchStftMixed(dSig, dOut, m.plan, signals, (uint32_t)frames, sigLen, sigLen, hop, center,
+                                     dWindow, m.tw, impl_->twReal[n], stream))
+            return -5;
+        return 0;
+    }
     if (prepareC2C(n / 2, kColsE) || prepareReal(n)) return -2;
     if (backend::launchStft(dSig, dOut, n, signals, (uint32_t)frames, sigLen, sigLen, hop, center, dWindow,
                             impl_->twC2C[{n / 2, kColsE}], impl_->twReal[n], stream))
@@ -780,6 +793,12 @@ int Plan::execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
                   float sInt, void* stream) {
     if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull) return -8;
     if (!validShape(n, (uint32_t)batch, kExecR2C)) return -8;
+    if (!pow2(n)) {   // even n, n/2 13-smooth: mixed-radix passes of n/2
+        if (prepareMixed(n / 2) || prepareReal(n)) return -2;
+        const auto& m = impl_->mixed[n / 2];
+        if (backend::launchR2CMixed(dIn, dOut, m.plan, batch, m.tw, impl_->twReal[n], sEdge, sInt, stream)) return -5;
+        return 0;
+    }
     int e = 0, cta = 0;
     if (resolve(backend::kR2C, n, &e, &cta)) return -1;
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;
@@ -794,6 +813,13 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
                   float sInt, float outScale, void* stream) {
     if (!dIn || !dOut || batch == 0 || batch > 0xFFFFFFFFull) return -8;
     if (!validShape(n, (uint32_t)batch, kExecC2R)) return -8;
+    if (!pow2(n)) {   // even n, n/2 13-smooth: mixed-radix passes of n/2
+        if (prepareMixed(n / 2) || prepareReal(n)) return -2;
+        const auto& m = impl_->mixed[n / 2];
+        if (backend::launchC2RMixed(dIn, dOut, m.plan, batch, m.tw, impl_->twReal[n], sEdge, sInt, outScale, stream))
+            return -5;
+        return 0;
+    }
     int e = 0, cta = 0;
     if (resolve(backend::kC2R, n, &e, &cta)) return -1;
     if (prepareC2C(n / 2, e) || prepareReal(n)) return -2;

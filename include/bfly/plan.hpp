@@ -229,7 +229,7 @@ public:
     int execC2CAxis(const void* dIn, void* dOut, uint32_t n, uint64_t outer, uint64_t inner,
                     int direction, float scale, void* stream);
     // STFT of `signals` contiguous real signals of sigLen fp32 samples: frames of n samples
-    // (n a power of two in [64, 8192]) every `hop`, centred with reflect padding when
+    // (n a power of two in [64, 8192], or even with n/2 13-smooth) every `hop`, centred with reflect padding when
     // `center` (then sigLen > n/2), times dWindow (n floats, or null), R2C of every frame into
     // dOut = [signals][frames][n/2+1] complex, frames = center ? 1 + sigLen/hop
     // : 1 + (sigLen-n)/hop.  *framesOut receives the frame count (may be null).
@@ -243,7 +243,9 @@ public:
     int execIstft(const void* dSpec, void* dOut, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
                   bool center, const void* dWindow, uint64_t outLen, float scale, void* stream);
     // R2C [batch][n] -> [batch][n/2+1] complex, bins scaled by (sEdge at 0 and n/2, sInt
-    // elsewhere); sEdge = sInt = 1 is the plain transform.
+    // elsewhere); sEdge = sInt = 1 is the plain transform.  n a power of two in [64, 8192]
+    // (single-pass team kernels), or even with n/2 = 2^a 3^b 5^c 7^d 11^e 13^f <= 12288
+    // (mixed-radix passes of n/2 with the split fused); the same lengths for execC2R.
     int execR2C(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float sEdge,
                 float sInt, void* stream);
     // C2R [batch][n/2+1] -> [batch][n]; input bins scaled by sEdge/sInt, output by outScale

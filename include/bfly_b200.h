@@ -159,7 +159,7 @@ int bfly_plan_exec_c2c_axis_async(bfly_plan* plan, const void* d_in, void* d_out
                                   uint64_t outer, uint64_t inner, int direction, float scale,
                                   void* stream);
 /* New: STFT of `signals` contiguous fp32 signals of sig_len samples: frames of n samples (n a
- * power of two in [64, 8192]) every `hop`, centred with reflect padding when center != 0
+ * power of two in [64, 8192], or even with n/2 13-smooth up to 24576) every `hop`, centred with reflect padding when center != 0
  * (sig_len > n/2; torch.stft's defaults), times d_window (n floats, or NULL), one-sided
  * spectrum of every frame into d_out = [signals][frames][n/2+1] complex;
  * frames = center ? 1 + sig_len/hop : 1 + (sig_len-n)/hop, returned in *frames (may be NULL).
@@ -176,12 +176,13 @@ int bfly_plan_exec_stft_async(bfly_plan* plan, const void* d_sig, void* d_out, u
 int bfly_plan_exec_istft_async(bfly_plan* plan, const void* d_spec, void* d_out, uint32_t n,
                                uint64_t signals, uint32_t frames, uint32_t hop, int center,
                                const void* d_window, uint64_t out_len, float scale, void* stream);
-/* R2C [batch][n] -> [batch][n/2+1] complex, n in [64, 8192]; bins 0 and n/2 scaled by
- * s_edge, the others by s_int (1, 1 for the plain transform). */
+/* R2C [batch][n] -> [batch][n/2+1] complex, n a power of two in [64, 8192], or even with n/2
+ * = 2^a 3^b 5^c 7^d 11^e 13^f up to 12288 (mixed-radix passes; the reference supports powers of
+ * two only); bins 0 and n/2 scaled by s_edge, the others by s_int (1, 1 for the plain transform). */
 int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, float s_edge, float s_int, void* stream);
-/* C2R [batch][n/2+1] -> [batch][n], n in [64, 8192]; input bins scaled by s_edge / s_int,
- * output by out_scale (1/n is numpy.fft.irfft). */
+/* C2R [batch][n/2+1] -> [batch][n], lengths as exec_r2c; input bins scaled by s_edge / s_int,
+ * output by out_scale (1/n is numpy.fft.irfft; imaginary parts of bins 0 and n/2 ignored). */
 int bfly_plan_exec_c2r_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, float s_edge, float s_int, float out_scale,
                              void* stream);

@@ -214,6 +214,61 @@ int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batc
     return 0;
 }
 
+// Real transforms of even n = 2M by direct DFTs (bins 0..M; weights as launchR2C / launchC2R).
+int launchR2CMixed(const void* in, void* out, const MixedRadix& half, uint64_t batch, const void*, const void*,
+                   float sEdge, float sInt, void*) {
+    if (!mixedRadix((uint32_t)half.n, nullptr)) return 1;
+    if (int r = launch()) return r;
+    const uint32_t m = (uint32_t)half.n, n = 2 * m;
+    std::vector<float> z(2 * n), spec(2 * n);
+    for (uint64_t b = 0; b < batch; ++b) {
+        const float* x = (const float*)in + b * n;
+        for (uint32_t j = 0; j < n; ++j) {
+            z[2 * j] = x[j];
+            z[2 * j + 1] = 0.f;
+        }
+        dft(z.data(), spec.data(), n, -1, 1.f);
+        float* o = (float*)out + b * 2 * (m + 1);
+        for (uint32_t k = 0; k <= m; ++k) {
+            const float w = (k == 0 || k == m) ? sEdge : sInt;
+            o[2 * k] = spec[2 * k] * w;
+            o[2 * k + 1] = spec[2 * k + 1] * w;
+        }
+    }
+    return 0;
+}
+int launchC2RMixed(const void* in, void* out, const MixedRadix& half, uint64_t batch, const void*, const void*,
+                   float sEdge, float sInt, float outScale, void*) {
+    if (!mixedRadix((uint32_t)half.n, nullptr)) return 1;
+    if (int r = launch()) return r;
+    c2rDirect(in, out, 2 * (uint32_t)half.n, batch, sEdge, sInt, outScale);
+    return 0;
+}
+int launchStftMixed(const void* sig, void* out, const MixedRadix& half, uint64_t signals, uint32_t framesPerSignal,
+                    uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window, const void*,
+                    const void*, void*) {
+    if (!mixedRadix((uint32_t)half.n, nullptr)) return 1;
+    if (int r = launch()) return r;
+    const uint32_t m = (uint32_t)half.n, n = 2 * m;
+    const float* x = (const float*)sig;
+    const float* w = (const float*)window;
+    std::vector<float> frame(2 * n), spec(2 * n);
+    for (uint64_t s = 0; s < signals; ++s)
+        for (uint32_t f = 0; f < framesPerSignal; ++f) {
+            const long long start = (long long)f * hop - (center ? m : 0);
+            for (uint32_t j = 0; j < n; ++j) {
+                long long i = start + j;
+                if (i < 0) i = -i;
+                if (i >= (long long)sigLen) i = 2 * ((long long)sigLen - 1) - i;
+                frame[2 * j] = x[s * sigStride + i] * (w ? w[j] : 1.f);
+                frame[2 * j + 1] = 0.f;
+            }
+            dft(frame.data(), spec.data(), n, -1, 1.f);
+            std::memcpy((float*)out + 2 * ((s * framesPerSignal + f) * (m + 1)), spec.data(), (m + 1) * 8);
+        }
+    return 0;
+}
+
 bool hasStft(uint32_t n) { return n >= kStftMinN && n <= kStftMaxN && !(n & (n - 1)); }
 int launchStft(const void* sig, void* out, uint32_t n, uint64_t signals, uint32_t framesPerSignal,
                uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,

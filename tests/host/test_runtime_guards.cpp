@@ -443,7 +443,7 @@ int main(int argc, char** argv) {
         CHECK(plan->execC2CAxis(d, d, 100, 1, 3, -1, 1.f, nullptr) == -8);
         CHECK(plan->execR2C2D(nullptr, d, 32, 64, 1, 1.f, nullptr) == -8);
         CHECK(plan->execR2C2D(d, d, 48, 64, 1, 1.f, nullptr) == -8);        // ny not a power of two
-        CHECK(plan->execR2C2D(d, d, 32, 96, 1, 1.f, nullptr) == -8);        // nx outside R2C
+        CHECK(plan->execR2C2D(d, d, 32, 34, 1, 1.f, nullptr) == -8);        // nx outside R2C (17 is not 13-smooth)
         CHECK(plan->execC2R2D(d, d, 8192, 64, 1, 1.f, nullptr) == -8);      // ny above 4096
         CHECK(plan->execC2R2D(d, d, 32, 16384, 1, 1.f, nullptr) == -8);     // nx outside C2R
         CHECK(plan->execC2R2D(d, d, 32, 64, 0, 1.f, nullptr) == -8);
@@ -485,7 +485,7 @@ int main(int argc, char** argv) {
         float* d = sig.data();
         uint64_t fr = 0;
         CHECK(plan->execStft(nullptr, d, 64, 1, 200, 16, true, nullptr, &fr, nullptr) == -8);
-        CHECK(plan->execStft(d, d, 96, 1, 200, 16, true, nullptr, &fr, nullptr) == -8);     // not a power of two
+        CHECK(plan->execStft(d, d, 34, 1, 200, 16, true, nullptr, &fr, nullptr) == -8);     // 17 is not 13-smooth
         CHECK(plan->execStft(d, d, 32, 1, 200, 16, true, nullptr, &fr, nullptr) == -8);     // below 64
         CHECK(plan->execStft(d, d, 16384, 1, 20000, 16, true, nullptr, &fr, nullptr) == -8);
         CHECK(plan->execStft(d, d, 64, 1, 200, 0, true, nullptr, &fr, nullptr) == -8);      // hop 0
@@ -493,6 +493,37 @@ int main(int argc, char** argv) {
         CHECK(plan->execStft(d, d, 64, 1, 32, 16, true, nullptr, &fr, nullptr) == -8);      // reflect needs len > n/2
         CHECK(plan->execStft(d, d, 64, 1, 63, 16, false, nullptr, &fr, nullptr) == -8);     // shorter than a frame
         CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
+    }
+
+    {   // real transforms of even non-power-of-two n (n/2 13-smooth): R2C matches a direct DFT,
+        // C2R (1/n) brings the signal back, each one launch once the tables exist
+        const uint32_t n = 96;
+        const uint64_t batch = 3;
+        std::vector<float> x(n * batch), back(n * batch), spec(2 * (n / 2 + 1) * batch);
+        for (size_t i = 0; i < x.size(); ++i) x[i] = (float)std::sin(0.37 * i + std::cos(0.11 * i));
+        CHECK(plan->execR2C(x.data(), spec.data(), n, batch, 1.f, 1.f, nullptr) == 0);
+        const int l0 = fake::launches;
+        CHECK(plan->execR2C(x.data(), spec.data(), n, batch, 1.f, 1.f, nullptr) == 0);
+        CHECK(fake::launches == l0 + 1);
+        double e = 0;
+        for (uint64_t b = 0; b < batch; ++b)
+            for (uint32_t k = 0; k <= n / 2; ++k) {
+                double re = 0, im = 0;
+                for (uint32_t j = 0; j < n; ++j) {
+                    const double a = -2 * M_PI * (double)((j * k) % n) / n;
+                    re += x[b * n + j] * std::cos(a);
+                    im += x[b * n + j] * std::sin(a);
+                }
+                const size_t o = 2 * (b * (n / 2 + 1) + k);
+                e = std::max(e, std::max(std::fabs(spec[o] - re), std::fabs(spec[o + 1] - im)));
+            }
+        CHECK(e < 1e-3);
+        CHECK(plan->execC2R(spec.data(), back.data(), n, batch, 1.f, 1.f, 1.f / n, nullptr) == 0);
+        e = 0;
+        for (size_t i = 0; i < x.size(); ++i) e = std::max(e, (double)std::fabs(back[i] - x[i]));
+        CHECK(e < 1e-4);
+        CHECK(plan->execR2C(x.data(), spec.data(), 34, batch, 1.f, 1.f, nullptr) == -8);   // 17 is not 13-smooth
+        CHECK(plan->execC2R(spec.data(), back.data(), 97, batch, 1.f, 1.f, 1.f, nullptr) == -8);   // odd
     }
 
     {   // inverse STFT: STFT then ISTFT gives the signal back (Hann window, centred, hop n/4),

@@ -103,7 +103,7 @@ def test_stft_rejects_unsupported(cuda):
     import bfly
     x = torch.randn(1000, device=cuda)
     with pytest.raises(bfly.BflyError):
-        bfly.stft(x, 96)                       # not a power of two
+        bfly.stft(x, 34)                       # even, but 17 is not 13-smooth
     with pytest.raises(ValueError):
         bfly.stft(x, 256, pad_mode="constant")
     with pytest.raises(ValueError):
