@@ -176,6 +176,12 @@ int launchC2RMixed(const void* in, void* out, const MixedRadix& half, uint64_t b
 int launchStftMixed(const void* sig, void* out, const MixedRadix& half, uint64_t signals, uint32_t framesPerSignal,
                     uint64_t sigLen, uint64_t sigStride, uint32_t hop, bool center, const void* window,
                     const void* tw, const void* twr, void* stream);
+// Inverse STFT of even non-power-of-two n <= kIstftMixedMaxN (n/2 13-smooth): the single
+// kernel of launchIstft on the mixed-radix passes (arguments as launchIstft).
+constexpr uint32_t kIstftMixedMaxN = 8192;
+int launchIstftMixed(const void* spec, void* out, const MixedRadix& half, uint64_t signals, uint32_t frames,
+                     uint32_t hop, int64_t start, uint64_t outLen, const void* window, const void* tw, const void* twr,
+                     float scale, void* stream);
 
 // STFT: `signals` real signals of sigLen samples (signal s at s*sigStride floats), frames of n
 // samples every `hop` (centred with reflect padding when `center`), times `window` (n floats,

@@ -256,6 +256,161 @@ __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__
     }
 }
 
+// Inverse STFT of even non-power-of-two N = 2M (M 13-smooth) in one kernel, with the work split,
+// carry and envelope of k_istft (k_stft.cu): CTA (s, c) owns the padded samples of Q hops of
+// signal s and transforms the frames covering them in waves of `rows` frames.  Per wave each
+// row stages its frame's un-split spectrum (c2r_split, out_scale) in buf1, runs the M-point
+// inverse passes into its natural-order row buffer, and all threads then overlap-add
+// w[j] * frame[j] over the wave's span (VEC = 4: four samples per thread), storing complete
+// samples times 1 / envelope and carrying the rest.
+template <bool WIDE, int VEC>
+__global__ void __launch_bounds__(512, 2) k_istft_mixed(const float2* __restrict__ spec, float* __restrict__ out,
+                                                        const float2* __restrict__ tw, const float2* __restrict__ twr,
+                                                        const float* __restrict__ window, MixedArgs a, uint32_t frames,
+                                                        uint32_t hop, uint32_t Q, uint32_t segs, int64_t start,
+                                                        uint64_t outLen, float out_scale, int T, int rows, int len) {
+    extern __shared__ float2 smem[];
+    const int CTA = T * rows;
+    const int rl = threadIdx.x / T;
+    const int t = threadIdx.x - rl * T;
+    const int M = a.n, N = 2 * M;
+    const uint32_t s = blockIdx.x / segs;
+    const uint32_t c = blockIdx.x - s * segs;
+    const int K = (N + (int)hop - 1) / (int)hop;
+    const int CARRY = N - (int)hop;
+    const int64_t padded = (int64_t)N + (int64_t)hop * (frames - 1);
+    const uint64_t first = (uint64_t)c * Q;
+    const uint32_t fA = first >= (uint64_t)(K - 1) ? (uint32_t)(first - (K - 1)) : 0u;
+    const uint32_t fB = (uint32_t)min((uint64_t)frames, first + Q);
+    const int64_t P0 = (int64_t)first * hop;
+    const int64_t end = start + (int64_t)outLen;
+    const int64_t P1 = c + 1 == segs ? (padded > end ? padded : end) : (int64_t)fB * hop;
+    const float2* src0 = spec + (uint64_t)s * frames * (M + 1);
+    float* dst = out + (uint64_t)s * outLen;
+    float2* buf0 = smem + (size_t)rl * 2 * len;
+    float2* buf1 = buf0 + len;
+    const int finOff = ((a.passes - 1) & 1) ? len : 0;   // buffer the last pass writes
+    auto frameOf = [&](int r) { return reinterpret_cast<const float*>(smem + (size_t)r * 2 * len + finOff); };
+    float* cur = reinterpret_cast<float*>(smem + (size_t)rows * 2 * len);
+    float* nxt = cur + CARRY;
+    float* rinv = nxt + CARRY;
+    for (int q = threadIdx.x; q < CARRY; q += CTA) cur[q] = 0.f;
+    for (int r = threadIdx.x; r < (int)hop; r += CTA) {
+        float e = 0.f;
+        for (int j = r; j < N; j += (int)hop) {
+            const float w = window ? __ldg(window + j) : 1.f;
+            e += w * w;
+        }
+        rinv[r] = e > 0.f ? 1.f / e : 0.f;
+    }
+    auto edgeInv = [&](int64_t p) {
+        float e = 0.f;
+        const int64_t fh = p / hop;
+        for (int64_t f = fh - K + 1 > 0 ? fh - K + 1 : 0; f <= fh && f < (int64_t)frames; ++f) {
+            const int64_t j = p - f * hop;
+            if (j < N) {
+                const float w = window ? __ldg(window + j) : 1.f;
+                e += w * w;
+            }
+        }
+        return e > 0.f ? 1.f / e : 0.f;
+    };
+    const int stepH = VEC * CTA / (int)hop, stepR = VEC * CTA - stepH * (int)hop;
+    const int qh0 = VEC * (int)threadIdx.x / (int)hop, qr0 = VEC * (int)threadIdx.x - qh0 * (int)hop;
+    auto clampq = [](int64_t v, int hi) { return (int)(v < 0 ? 0 : (v > hi ? hi : v)); };
+
+    for (uint32_t f0 = fA; f0 < fB; f0 += rows) {
+        const int R = (int)min((uint32_t)rows, fB - f0);
+        __syncthreads();   // the previous wave is done with the row buffers and the carry
+        // rows past R (a CTA's partial first or last wave) transform frame f0 again, unread
+        const float2* src = src0 + (uint64_t)(f0 + (rl < R ? rl : 0)) * (M + 1);
+        for (int k = t; k < M; k += T)
+            buf1[k] = c2r_split(ld_stream(src + k), ld_stream(src + (k == 0 ? M : M - k)), k, __ldg(twr + k), 1.f, 1.f,
+                                out_scale);
+        __syncthreads();
+        mixed_row<true, WIDE, false, false>(a, nullptr, nullptr, buf0, buf1, tw, true, t, T, 1.f);
+        __syncthreads();
+        const bool tail = f0 + R == frames;
+        const int span = (R - 1) * (int)hop + N;
+        const int done = tail ? span : R * (int)hop;
+        const int64_t base = (int64_t)f0 * hop;
+        const int wlo = clampq((P0 > start ? P0 : start) - base, done);
+        const int whi = clampq((P1 < end ? P1 : end) - base, done);
+        const int elo = clampq((int64_t)(N - 1) - base, span);
+        const int ehi = clampq((int64_t)frames * hop - base, span);
+        float* dq = dst + (base - start);   // output of span offset q at dq[q] (wlo <= q < whi)
+        int qh = qh0, qr = qr0;
+        if constexpr (VEC == 1) {
+            for (int q = threadIdx.x; q < span; q += CTA) {
+                float val = q < CARRY ? cur[q] : 0.f;
+                const int rlo = qh - K + 1 > 0 ? qh - K + 1 : 0;
+                const int rhi = qh < R - 1 ? qh : R - 1;
+                for (int r = rlo; r <= rhi; ++r) {
+                    const int j = qr + (qh - r) * (int)hop;
+                    if (j < N) val += (window ? __ldg(window + j) : 1.f) * frameOf(r)[j];
+                }
+                if (q >= done) {
+                    nxt[q - done] = val;
+                } else if (q >= wlo && q < whi) {
+                    __stcs(dq + q, val * (q >= elo && q < ehi ? rinv[qr] : edgeInv(base + q)));
+                }
+                qh += stepH;
+                qr += stepR;
+                if (qr >= (int)hop) {
+                    qr -= (int)hop;
+                    ++qh;
+                }
+            }
+        } else {
+            // hop, N, CARRY, done, wlo, whi, len are multiples of 4 and the 4 samples share q / hop
+            for (int q = 4 * threadIdx.x; q < span; q += 4 * CTA) {
+                float4 val = q < CARRY ? *reinterpret_cast<const float4*>(cur + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const int rlo = qh - K + 1 > 0 ? qh - K + 1 : 0;
+                const int rhi = qh < R - 1 ? qh : R - 1;
+                for (int r = rlo; r <= rhi; ++r) {
+                    const int j = qr + (qh - r) * (int)hop;
+                    if (j < N) {
+                        const float4 x = *reinterpret_cast<const float4*>(frameOf(r) + j);
+                        const float4 w = window ? __ldg(reinterpret_cast<const float4*>(window + j))
+                                                : make_float4(1.f, 1.f, 1.f, 1.f);
+                        val.x = fmaf(w.x, x.x, val.x);
+                        val.y = fmaf(w.y, x.y, val.y);
+                        val.z = fmaf(w.z, x.z, val.z);
+                        val.w = fmaf(w.w, x.w, val.w);
+                    }
+                }
+                if (q >= done) {
+                    *reinterpret_cast<float4*>(nxt + q - done) = val;
+                } else if (q >= wlo && q < whi) {
+                    float4 e;
+                    if (q >= elo && q + 3 < ehi) {
+                        e = *reinterpret_cast<const float4*>(rinv + qr);
+                    } else {
+                        auto inv = [&](int u) { return q + u >= elo && q + u < ehi ? rinv[qr + u] : edgeInv(base + q + u); };
+                        e = make_float4(inv(0), inv(1), inv(2), inv(3));
+                    }
+                    __stcs(reinterpret_cast<float4*>(dq + q), make_float4(val.x * e.x, val.y * e.y, val.z * e.z, val.w * e.w));
+                }
+                qh += stepH;
+                qr += stepR;
+                if (qr >= (int)hop) {
+                    qr -= (int)hop;
+                    ++qh;
+                }
+            }
+        }
+        float* sw = cur;
+        cur = nxt;
+        nxt = sw;
+    }
+    if (c + 1 == segs) {   // samples past the last frame up to outLen are zero
+        for (int64_t p = (padded > P0 ? padded : P0) + threadIdx.x; p < P1; p += CTA) {
+            const int64_t i = p - start;
+            if (i >= 0 && i < (int64_t)outLen) __stcs(dst + i, 0.f);
+        }
+    }
+}
+
 // tw[twoff[p] + (r-1) Ns + k] = W_(Ns R)^(k r) = W_n^(k r n / (Ns R)) in FP64, rounded once.
 static __global__ void k_tw_mixed(float2* __restrict__ tw, MixedArgs a, int total) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -403,6 +558,42 @@ int launchStftMixed(const void* sig, void* out, const MixedRadix& half, uint64_t
         static_cast<const float*>(sig), static_cast<float2*>(out), static_cast<const float2*>(tw),
         static_cast<const float2*>(twr), static_cast<const float*>(window), m.args, frames, framesPerSignal,
         (int64_t)sigLen, sigStride, hop, center ? 1 : 0, m.T, m.rows, m.len);
+    return (int)cudaGetLastError();
+}
+
+int launchIstftMixed(const void* spec, void* out, const MixedRadix& half, uint64_t signals, uint32_t frames,
+                     uint32_t hop, int64_t start, uint64_t outLen, const void* window, const void* tw, const void* twr,
+                     float scale, void* stream) {
+    if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
+    const int N = 2 * half.n;
+    if (N > (int)kIstftMixedMaxN || hop == 0 || hop > (uint32_t)N || frames == 0) return (int)cudaErrorInvalidValue;
+    MixedShape m = mixedShape(half);
+    m.len += m.len & 1;   // even: every row buffer 16-byte aligned for the float4 overlap-add
+    const int smem = m.rows * 2 * m.len * 8 + (2 * (N - (int)hop) + (int)hop) * 4;
+    // opted in once per kernel at the largest case: rows * 2 * len of the longest plan plus
+    // carry and envelope of N = kIstftMixedMaxN
+    constexpr int kMaxSmem = 227 * 1024;
+    if (smem > kMaxSmem) return (int)cudaErrorInvalidValue;
+    // float4 overlap-add: frame, hop and output lengths multiples of 4, 16-byte aligned output
+    // and window (a frame of N % 4 == 2 would read past its row)
+    const bool vec = N % 4 == 0 && hop % 4 == 0 && outLen % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15u) == 0 &&
+                     (reinterpret_cast<uintptr_t>(window) & 15u) == 0;
+    auto* fn = m.wide ? (vec ? dev::k_istft_mixed<true, 4> : dev::k_istft_mixed<true, 1>)
+                      : (vec ? dev::k_istft_mixed<false, 4> : dev::k_istft_mixed<false, 1>);
+    if (int e = optInSharedMemory((const void*)fn, kMaxSmem)) return e;
+    int device = 0, sms = 0, perSm = 0;
+    if (cudaGetDevice(&device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, m.T * m.rows, smem) != cudaSuccess || perSm < 1)
+        return (int)cudaErrorInvalidConfiguration;
+    uint32_t q, segs;
+    istftSegments((uint32_t)N, m.rows, frames, hop, signals, (uint64_t)sms * perSm, &q, &segs);
+    const uint64_t grid = signals * segs;
+    if (grid > 0x7fffffffull) return (int)cudaErrorInvalidValue;
+    fn<<<(unsigned)grid, m.T * m.rows, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<const float2*>(spec), static_cast<float*>(out), static_cast<const float2*>(tw),
+        static_cast<const float2*>(twr), static_cast<const float*>(window), m.args, frames, hop, q, segs, start,
+        outLen, scale / N, m.T, m.rows, m.len);
     return (int)cudaGetLastError();
 }
 

@@ -779,9 +779,19 @@ int Plan::execStft(const void* dSig, void* dOut, uint32_t n, uint64_t signals, u
 
 int Plan::execIstft(const void* dSpec, void* dOut, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
                     bool center, const void* dWindow, uint64_t outLen, float scale, void* stream) {
-    if (!impl_ || !dSpec || !dOut || signals == 0 || frames == 0 || hop == 0 || hop > n || !backend::hasStft(n))
+    const bool mixedN = !pow2(n) && realMixed(n) && n <= backend::kIstftMixedMaxN;
+    if (!impl_ || !dSpec || !dOut || signals == 0 || frames == 0 || hop == 0 || hop > n ||
+        !(backend::hasStft(n) || mixedN))
         return -8;
     if (signals * frames > 0xFFFFFFFFull || outLen == 0 || outLen > (1ull << 62)) return -8;
+    if (mixedN) {
+        if (prepareMixed(n / 2) || prepareReal(n)) return -2;
+        const auto& m = impl_->mixed[n / 2];
+        if (backend::launchIstftMixed(dSpec, dOut, m.plan, signals, frames, hop, center ? (int64_t)(n / 2) : 0, outLen,
+                                      dWindow, m.tw, impl_->twReal[n], scale, stream))
+            return -5;
+        return 0;
+    }
     if (prepareC2C(n / 2, kColsE) || prepareReal(n)) return -2;
     if (backend::launchIstft(dSpec, dOut, n, signals, frames, hop, center ? (int64_t)(n / 2) : 0, outLen, dWindow,
                              impl_->twC2C[{n / 2, kColsE}], impl_->twReal[n], scale, stream))

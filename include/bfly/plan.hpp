@@ -238,8 +238,9 @@ public:
     // Inverse STFT (torch.istft): dSpec = [signals][frames][n/2+1] complex -> dOut =
     // [signals][outLen] fp32 in one kernel: every frame inverse-transformed (1/n), windowed and
     // overlap-added, out[i] = sum_f w[j] frame_f[j] / sum_f w[j]^2 at padded position
-    // i + (center ? n/2 : 0), times `scale`; hop <= n.  Samples with a zero window envelope, and
-    // those past the last frame, are 0.
+    // i + (center ? n/2 : 0), times `scale`; hop <= n; n a power of two in [64, 8192] or even
+    // with n/2 13-smooth up to 8192.  Samples with a zero window envelope, and those past the
+    // last frame, are 0.
     int execIstft(const void* dSpec, void* dOut, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
                   bool center, const void* dWindow, uint64_t outLen, float scale, void* stream);
     // R2C [batch][n] -> [batch][n/2+1] complex, bins scaled by (sEdge at 0 and n/2, sInt

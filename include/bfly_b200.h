@@ -168,7 +168,8 @@ int bfly_plan_exec_c2c_axis_async(bfly_plan* plan, const void* d_in, void* d_out
 int bfly_plan_exec_stft_async(bfly_plan* plan, const void* d_sig, void* d_out, uint32_t n,
                               uint64_t signals, uint64_t sig_len, uint32_t hop, int center,
                               const void* d_window, uint64_t* frames, void* stream);
-/* New: inverse STFT (torch.istft): d_spec = [signals][frames][n/2+1] complex64 -> d_out =
+/* New: inverse STFT (torch.istft), n a power of two in [64, 8192] or even with n/2 13-smooth up
+ * to 8192: d_spec = [signals][frames][n/2+1] complex64 -> d_out =
  * [signals][out_len] fp32: every frame inverse-transformed (1/n), then overlap-added with the
  * window (d_window, n floats, or NULL) and divided by the overlap-added squared window, from
  * padded position n/2 when center != 0, times scale; hop <= n; samples whose window envelope

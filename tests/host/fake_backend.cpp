@@ -303,10 +303,26 @@ void istftSegments(uint32_t n, int rows, uint32_t frames, uint32_t hop, uint64_t
 }
 
 // C2R of every frame (scale/n), windowed overlap-add, division by the squared-window envelope.
+static void istftDirect(const void* spec, void* out, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
+                        int64_t start, uint64_t outLen, const void* window, float scale);
+int launchIstftMixed(const void* spec, void* out, const MixedRadix& half, uint64_t signals, uint32_t frames,
+                     uint32_t hop, int64_t start, uint64_t outLen, const void* window, const void*, const void*,
+                     float scale, void*) {
+    const uint32_t n = 2 * (uint32_t)half.n;
+    if (!mixedRadix((uint32_t)half.n, nullptr) || n > kIstftMixedMaxN || hop == 0 || hop > n || frames == 0) return 1;
+    if (int r = launch()) return r;
+    istftDirect(spec, out, n, signals, frames, hop, start, outLen, window, scale);
+    return 0;
+}
 int launchIstft(const void* spec, void* out, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
                 int64_t start, uint64_t outLen, const void* window, const void*, const void*, float scale, void*) {
     if (!hasStft(n) || hop == 0 || hop > n || frames == 0) return 1;
     if (int r = launch()) return r;
+    istftDirect(spec, out, n, signals, frames, hop, start, outLen, window, scale);
+    return 0;
+}
+static void istftDirect(const void* spec, void* out, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
+                        int64_t start, uint64_t outLen, const void* window, float scale) {
     const float* w = (const float*)window;
     std::vector<float> fr((size_t)frames * n);
     for (uint64_t s = 0; s < signals; ++s) {
@@ -324,7 +340,6 @@ int launchIstft(const void* spec, void* out, uint32_t n, uint64_t signals, uint3
             ((float*)out)[s * outLen + i] = env > 0 ? (float)(acc / env) : 0.f;
         }
     }
-    return 0;
 }
 
 bool hasCols(uint32_t ny) { return ny >= 32 && ny <= 4096 && !(ny & (ny - 1)); }

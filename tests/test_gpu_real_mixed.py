@@ -1,7 +1,7 @@
 """Real transforms of even non-power-of-two lengths (n = 2M, M 13-smooth) on the mixed-radix
 passes: R2C / C2R against FP64 numpy.rfft / irfft, their adjoints against torch.fft's
-gradients, STFT against torch.stft (n_fft = 400 with hop 160 is the common speech front-end),
-and the 2-D real transforms whose rows take this path.  Tolerance: rel L2 <= 1e-6 per row (the
+gradients, STFT and inverse STFT against torch.stft / torch.istft (n_fft = 400 with hop 160 is
+the common speech front-end), and the 2-D real transforms whose rows take this path.  Tolerance: rel L2 <= 1e-6 per row (the
 R2C / C2R gate), 2e-6 against torch, 1e-5 for gradients."""
 import numpy as np
 import pytest
@@ -113,3 +113,41 @@ def test_real_2d_mixed_rows(plan, cuda):
     assert plan.exec_c2r_2d(X.data_ptr(), y.data_ptr(), ny, nx, batch, 1.0 / (ny * nx), 0) == 0
     torch.cuda.synchronize()
     assert (torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x)).item() <= 4e-6
+
+
+@pytest.mark.parametrize("n_fft,hop,center,length", [(400, 160, True, None), (480, 120, True, 15000), (150, 37, True, None),
+                                                     (1000, 250, False, None), (6000, 1500, True, None), (400, 100, True, 16003)])
+def test_istft_mixed_matches_torch(cuda, n_fft, hop, center, length):
+    """One kernel for even non-power-of-two n_fft: float4 overlap-add where n_fft, hop and the
+    output length are multiples of 4, scalar otherwise (150 and hop 37)."""
+    import torch
+    import bfly
+    g = torch.Generator(device=cuda).manual_seed(n_fft + hop)
+    x = torch.randn(2, 16000, device=cuda, generator=g)
+    w = torch.hann_window(n_fft, device=cuda) + (0.0 if center else 0.1)
+    spec = torch.stft(x, n_fft, hop_length=hop, window=w, center=center, return_complex=True)
+    ref = torch.istft(spec, n_fft, hop_length=hop, window=w, center=center, length=length)
+    got = bfly.istft(spec, n_fft, hop_length=hop, window=w, center=center, length=length)
+    assert got.shape == ref.shape
+    assert (torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)).item() <= 5e-6
+    back = bfly.istft(bfly.stft(x, n_fft, hop_length=hop, window=w, center=center), n_fft, hop_length=hop,
+                      window=w, center=center, length=x.shape[-1] if center else None)
+    if center:
+        assert (torch.linalg.vector_norm(back - x) / torch.linalg.vector_norm(x)).item() <= 4e-6
+
+
+def test_istft_mixed_autograd(cuda):
+    import torch
+    import bfly
+    g = torch.Generator(device=cuda).manual_seed(21)
+    w = torch.hann_window(400, device=cuda) + 0.1
+    spec0 = torch.stft(torch.randn(2, 6000, device=cuda, generator=g), 400, hop_length=160, window=w,
+                       return_complex=True)
+    sa = spec0.clone().requires_grad_(True)
+    sb = spec0.clone().requires_grad_(True)
+    ya = bfly.istft(sa, 400, hop_length=160, window=w, length=5900)
+    yb = torch.istft(sb, 400, hop_length=160, window=w, length=5900)
+    wt = torch.rand(ya.shape, device=cuda, generator=g)
+    (wt * ya * ya).sum().backward()
+    (wt * yb * yb).sum().backward()
+    assert (torch.linalg.vector_norm(sa.grad - sb.grad) / torch.linalg.vector_norm(sb.grad)).item() <= 1e-5
