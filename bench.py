@@ -416,7 +416,7 @@ def extra_measurements(dev, stream):
     # 2^24 samples, centred; bytes counted per frame as the reference's dense-frame R2C proxy
     out["stft"] = {}
     plan = bfly.plan_for(dev, 1024, "real")
-    for n, hop in ((256, 64), (1024, 256), (4096, 1024)):
+    for n, hop in ((256, 64), (1024, 256), (4096, 1024), (400, 160)):
         L, S = 1 << 24, 4
         g = torch.Generator(device=dev).manual_seed(n)
         x = torch.randn(S, L, device=dev, generator=g)
@@ -443,7 +443,7 @@ def extra_measurements(dev, stream):
                                                     "istft_ms": round(ms_i, 4), "round_trip_rel_l2": rt}
         del x, y, xb
     # ---- real transforms: R2C forward and its adjoint (weighted C2R), batch 1024
-    for n in (128, 1024, 4096, 8192):
+    for n in (128, 1024, 4096, 8192, 400, 1000):
         b = 1024
         g = torch.Generator(device=dev).manual_seed(n)
         x = torch.rand(b, n, device=dev, generator=g) * 2 - 1
