@@ -17,6 +17,7 @@
 #include "backend.h"
 #include "fft_kernels.cuh"
 #include "fft_odd.cuh"
+#include "istft_ola.cuh"
 
 namespace bfly {
 namespace dev {
@@ -236,9 +237,17 @@ __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__
             i = i >= sigLen ? 2 * (sigLen - 1) - i : i;
             return __ldg(x + i);
         };
+        // interior frames starting on an 8-byte boundary read one float2 per complex value; the
+        // others sample with reflection
+        const bool direct = start >= 0 && start + 2 * M <= sigLen && (reinterpret_cast<uintptr_t>(x + start) & 7u) == 0;
+        const float2* xv = reinterpret_cast<const float2*>(x + (direct ? start : 0));
+        const float2* wv = reinterpret_cast<const float2*>(window);
         for (int m = t; m < M; m += T) {
-            float2 z = make_float2(sample(start + 2 * m), sample(start + 2 * m + 1));
-            if (window) z = make_float2(z.x * __ldg(window + 2 * m), z.y * __ldg(window + 2 * m + 1));
+            float2 z = direct ? __ldg(xv + m) : make_float2(sample(start + 2 * m), sample(start + 2 * m + 1));
+            if (window) {
+                const float2 w = __ldg(wv + m);
+                z = make_float2(z.x * w.x, z.y * w.y);
+            }
             buf1[m] = z;
         }
     }
@@ -256,13 +265,10 @@ __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__
     }
 }
 
-// Inverse STFT of even non-power-of-two N = 2M (M 13-smooth) in one kernel, with the work split,
-// carry and envelope of k_istft (k_stft.cu): CTA (s, c) owns the padded samples of Q hops of
-// signal s and transforms the frames covering them in waves of `rows` frames.  Per wave each
-// row stages its frame's un-split spectrum (c2r_split, out_scale) in buf1, runs the M-point
-// inverse passes into its natural-order row buffer, and all threads then overlap-add
-// w[j] * frame[j] over the wave's span (VEC = 4: four samples per thread), storing complete
-// samples times 1 / envelope and carrying the rest.
+// Inverse STFT of even non-power-of-two N = 2M (M 13-smooth) in one kernel: per wave each row
+// stages its frame's un-split spectrum (c2r_split, out_scale) in buf1 and runs the M-point
+// inverse passes into its natural-order row buffer; the segment split, carry, envelope and
+// overlap-add (window applied there) are IstftSegment (istft_ola.cuh), as in k_istft.
 template <bool WIDE, int VEC>
 __global__ void __launch_bounds__(512, 2) k_istft_mixed(const float2* __restrict__ spec, float* __restrict__ out,
                                                         const float2* __restrict__ tw, const float2* __restrict__ twr,
@@ -270,57 +276,20 @@ __global__ void __launch_bounds__(512, 2) k_istft_mixed(const float2* __restrict
                                                         uint32_t hop, uint32_t Q, uint32_t segs, int64_t start,
                                                         uint64_t outLen, float out_scale, int T, int rows, int len) {
     extern __shared__ float2 smem[];
-    const int CTA = T * rows;
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
-    const int M = a.n, N = 2 * M;
-    const uint32_t s = blockIdx.x / segs;
-    const uint32_t c = blockIdx.x - s * segs;
-    const int K = (N + (int)hop - 1) / (int)hop;
-    const int CARRY = N - (int)hop;
-    const int64_t padded = (int64_t)N + (int64_t)hop * (frames - 1);
-    const uint64_t first = (uint64_t)c * Q;
-    const uint32_t fA = first >= (uint64_t)(K - 1) ? (uint32_t)(first - (K - 1)) : 0u;
-    const uint32_t fB = (uint32_t)min((uint64_t)frames, first + Q);
-    const int64_t P0 = (int64_t)first * hop;
-    const int64_t end = start + (int64_t)outLen;
-    const int64_t P1 = c + 1 == segs ? (padded > end ? padded : end) : (int64_t)fB * hop;
-    const float2* src0 = spec + (uint64_t)s * frames * (M + 1);
-    float* dst = out + (uint64_t)s * outLen;
+    const int M = a.n;
+    IstftSegment seg;
+    seg.init(2 * M, hop, frames, Q, segs, start, outLen, window, out,
+             reinterpret_cast<float*>(smem + (size_t)rows * 2 * len));
+    const float2* src0 = spec + (uint64_t)(blockIdx.x / segs) * frames * (M + 1);
     float2* buf0 = smem + (size_t)rl * 2 * len;
     float2* buf1 = buf0 + len;
     const int finOff = ((a.passes - 1) & 1) ? len : 0;   // buffer the last pass writes
     auto frameOf = [&](int r) { return reinterpret_cast<const float*>(smem + (size_t)r * 2 * len + finOff); };
-    float* cur = reinterpret_cast<float*>(smem + (size_t)rows * 2 * len);
-    float* nxt = cur + CARRY;
-    float* rinv = nxt + CARRY;
-    for (int q = threadIdx.x; q < CARRY; q += CTA) cur[q] = 0.f;
-    for (int r = threadIdx.x; r < (int)hop; r += CTA) {
-        float e = 0.f;
-        for (int j = r; j < N; j += (int)hop) {
-            const float w = window ? __ldg(window + j) : 1.f;
-            e += w * w;
-        }
-        rinv[r] = e > 0.f ? 1.f / e : 0.f;
-    }
-    auto edgeInv = [&](int64_t p) {
-        float e = 0.f;
-        const int64_t fh = p / hop;
-        for (int64_t f = fh - K + 1 > 0 ? fh - K + 1 : 0; f <= fh && f < (int64_t)frames; ++f) {
-            const int64_t j = p - f * hop;
-            if (j < N) {
-                const float w = window ? __ldg(window + j) : 1.f;
-                e += w * w;
-            }
-        }
-        return e > 0.f ? 1.f / e : 0.f;
-    };
-    const int stepH = VEC * CTA / (int)hop, stepR = VEC * CTA - stepH * (int)hop;
-    const int qh0 = VEC * (int)threadIdx.x / (int)hop, qr0 = VEC * (int)threadIdx.x - qh0 * (int)hop;
-    auto clampq = [](int64_t v, int hi) { return (int)(v < 0 ? 0 : (v > hi ? hi : v)); };
 
-    for (uint32_t f0 = fA; f0 < fB; f0 += rows) {
-        const int R = (int)min((uint32_t)rows, fB - f0);
+    for (uint32_t f0 = seg.fA; f0 < seg.fB; f0 += rows) {
+        const int R = (int)min((uint32_t)rows, seg.fB - f0);
         __syncthreads();   // the previous wave is done with the row buffers and the carry
         // rows past R (a CTA's partial first or last wave) transform frame f0 again, unread
         const float2* src = src0 + (uint64_t)(f0 + (rl < R ? rl : 0)) * (M + 1);
@@ -330,85 +299,15 @@ __global__ void __launch_bounds__(512, 2) k_istft_mixed(const float2* __restrict
         __syncthreads();
         mixed_row<true, WIDE, false, false>(a, nullptr, nullptr, buf0, buf1, tw, true, t, T, 1.f);
         __syncthreads();
-        const bool tail = f0 + R == frames;
-        const int span = (R - 1) * (int)hop + N;
-        const int done = tail ? span : R * (int)hop;
-        const int64_t base = (int64_t)f0 * hop;
-        const int wlo = clampq((P0 > start ? P0 : start) - base, done);
-        const int whi = clampq((P1 < end ? P1 : end) - base, done);
-        const int elo = clampq((int64_t)(N - 1) - base, span);
-        const int ehi = clampq((int64_t)frames * hop - base, span);
-        float* dq = dst + (base - start);   // output of span offset q at dq[q] (wlo <= q < whi)
-        int qh = qh0, qr = qr0;
-        if constexpr (VEC == 1) {
-            for (int q = threadIdx.x; q < span; q += CTA) {
-                float val = q < CARRY ? cur[q] : 0.f;
-                const int rlo = qh - K + 1 > 0 ? qh - K + 1 : 0;
-                const int rhi = qh < R - 1 ? qh : R - 1;
-                for (int r = rlo; r <= rhi; ++r) {
-                    const int j = qr + (qh - r) * (int)hop;
-                    if (j < N) val += (window ? __ldg(window + j) : 1.f) * frameOf(r)[j];
-                }
-                if (q >= done) {
-                    nxt[q - done] = val;
-                } else if (q >= wlo && q < whi) {
-                    __stcs(dq + q, val * (q >= elo && q < ehi ? rinv[qr] : edgeInv(base + q)));
-                }
-                qh += stepH;
-                qr += stepR;
-                if (qr >= (int)hop) {
-                    qr -= (int)hop;
-                    ++qh;
-                }
-            }
-        } else {
-            // hop, N, CARRY, done, wlo, whi, len are multiples of 4 and the 4 samples share q / hop
-            for (int q = 4 * threadIdx.x; q < span; q += 4 * CTA) {
-                float4 val = q < CARRY ? *reinterpret_cast<const float4*>(cur + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-                const int rlo = qh - K + 1 > 0 ? qh - K + 1 : 0;
-                const int rhi = qh < R - 1 ? qh : R - 1;
-                for (int r = rlo; r <= rhi; ++r) {
-                    const int j = qr + (qh - r) * (int)hop;
-                    if (j < N) {
-                        const float4 x = *reinterpret_cast<const float4*>(frameOf(r) + j);
-                        const float4 w = window ? __ldg(reinterpret_cast<const float4*>(window + j))
-                                                : make_float4(1.f, 1.f, 1.f, 1.f);
-                        val.x = fmaf(w.x, x.x, val.x);
-                        val.y = fmaf(w.y, x.y, val.y);
-                        val.z = fmaf(w.z, x.z, val.z);
-                        val.w = fmaf(w.w, x.w, val.w);
-                    }
-                }
-                if (q >= done) {
-                    *reinterpret_cast<float4*>(nxt + q - done) = val;
-                } else if (q >= wlo && q < whi) {
-                    float4 e;
-                    if (q >= elo && q + 3 < ehi) {
-                        e = *reinterpret_cast<const float4*>(rinv + qr);
-                    } else {
-                        auto inv = [&](int u) { return q + u >= elo && q + u < ehi ? rinv[qr + u] : edgeInv(base + q + u); };
-                        e = make_float4(inv(0), inv(1), inv(2), inv(3));
-                    }
-                    __stcs(reinterpret_cast<float4*>(dq + q), make_float4(val.x * e.x, val.y * e.y, val.z * e.z, val.w * e.w));
-                }
-                qh += stepH;
-                qr += stepR;
-                if (qr >= (int)hop) {
-                    qr -= (int)hop;
-                    ++qh;
-                }
-            }
-        }
-        float* sw = cur;
-        cur = nxt;
-        nxt = sw;
+        seg.wave<VEC, 0>(
+            f0, R, [&](int r, int j) { return (window ? __ldg(window + j) : 1.f) * frameOf(r)[j]; },
+            [&](int r, int j) {
+                const float4 x = *reinterpret_cast<const float4*>(frameOf(r) + j);
+                const float4 w = window ? __ldg(reinterpret_cast<const float4*>(window + j)) : make_float4(1.f, 1.f, 1.f, 1.f);
+                return make_float4(w.x * x.x, w.y * x.y, w.z * x.z, w.w * x.w);
+            });
     }
-    if (c + 1 == segs) {   // samples past the last frame up to outLen are zero
-        for (int64_t p = (padded > P0 ? padded : P0) + threadIdx.x; p < P1; p += CTA) {
-            const int64_t i = p - start;
-            if (i >= 0 && i < (int64_t)outLen) __stcs(dst + i, 0.f);
-        }
-    }
+    seg.zeroTail(segs);
 }
 
 // tw[twoff[p] + (r-1) Ns + k] = W_(Ns R)^(k r) = W_n^(k r n / (Ns R)) in FP64, rounded once.

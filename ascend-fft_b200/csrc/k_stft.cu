@@ -12,6 +12,7 @@
 
 #include "backend.h"
 #include "fft_kernels.cuh"
+#include "istft_ola.cuh"
 
 namespace bfly {
 namespace dev {
@@ -77,21 +78,11 @@ k_stft(const float* __restrict__ sig, float2* __restrict__ out, const float2* __
     if (t == 0) bin(M, wm);
 }
 
-// Inverse STFT in one kernel (torch.istft): every frame's C2R, window, overlap-add and the
-// division by the overlap-added squared window, each output sample written once.
-//   y[p] = sum_f w[j] x_f[j] / sum_f w[j]^2,  j = p - f*hop in [0, N),  x_f = out_scale * IDFT_N
-//   (spec[s][f]) with the imaginary parts of bins 0 and N/2 ignored;  out[s][i] = y[i + start],
-//   i < outLen, zero past the last frame.
-// CTA (s, c) owns padded samples [c*Q*hop, (c+1)*Q*hop) of signal s (the last CTA of a signal
-// also the tail).  It transforms frames c*Q - (K-1) .. (c+1)*Q - 1 (K = ceil(N/hop) frames cover
-// a sample) in waves of ROWS frames: each frame's C2R runs in registers, the windowed result
-// lands in the row's shared buffer, then all threads sum, per sample of the wave's span, the
-// carried partial sum of earlier frames and the wave's frames covering it.  Samples no later
-// frame touches are complete and stored, times 1 / envelope (a per-CTA table over p mod hop,
-// exact sums within a frame of either end); the rest (N - hop samples) are carried to the next
-// wave in the other half of a ping-pong buffer.  Frames before the CTA's first sample only fill
-// the carry, so K - 1 frames per CTA are transformed twice (Q is chosen so that costs < 7%).
-// Summation order is fixed (frames in increasing order), so results are deterministic.
+// Inverse STFT in one kernel (torch.istft) for power-of-two N: every frame's C2R in registers
+// (the k_c2r team), windowed into the row's shared buffer, ROWS frames per wave; the segment
+// split, carry, envelope and overlap-add are IstftSegment (istft_ola.cuh).  Frames before the
+// CTA's first sample only fill the carry, so K - 1 frames per CTA are transformed twice (Q is
+// chosen so that costs < 7%).
 // Row stride of the inverse-STFT row buffers: the team's exchange stride rounded up to even.
 template <int M, int E>
 __host__ __device__ constexpr int istft_row_stride() {
@@ -113,54 +104,14 @@ k_istft(const float2* __restrict__ spec, float* __restrict__ out, const float2* 
     extern __shared__ float2 smem[];
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
-    const uint32_t s = blockIdx.x / segs;
-    const uint32_t c = blockIdx.x - s * segs;
-    const int K = (N + (int)hop - 1) / (int)hop;
-    const int CARRY = N - (int)hop;
-    const int64_t padded = (int64_t)N + (int64_t)hop * (frames - 1);
-    const uint64_t first = (uint64_t)c * Q;
-    const uint32_t fA = first >= (uint64_t)(K - 1) ? (uint32_t)(first - (K - 1)) : 0u;
-    const uint32_t fB = (uint32_t)min((uint64_t)frames, first + Q);
-    const int64_t P0 = (int64_t)first * hop;
-    const int64_t end = start + (int64_t)outLen;
-    const int64_t P1 = c + 1 == segs ? (padded > end ? padded : end) : (int64_t)fB * hop;
-    const float2* src0 = spec + (uint64_t)s * frames * (M + 1);
-    float* dst = out + (uint64_t)s * outLen;
+    IstftSegment seg;
+    seg.init(N, hop, frames, Q, segs, start, outLen, window, out, reinterpret_cast<float*>(smem + ROWS * S));
+    const float2* src0 = spec + (uint64_t)(blockIdx.x / segs) * frames * (M + 1);
     float2* sm = smem + rl * S;
-    float* cur = reinterpret_cast<float*>(smem + ROWS * S);
-    float* nxt = cur + CARRY;
-    // 1 / (overlap-added squared window) of samples every frame slot of which exists
-    // (N-1 <= p < frames*hop): periodic in p with period hop
-    float* rinv = nxt + CARRY;
-    for (int q = threadIdx.x; q < CARRY; q += CTA) cur[q] = 0.f;
-    for (int r = threadIdx.x; r < (int)hop; r += CTA) {
-        float e = 0.f;
-        for (int j = r; j < N; j += (int)hop) {
-            const float w = window ? __ldg(window + j) : 1.f;
-            e += w * w;
-        }
-        rinv[r] = e > 0.f ? 1.f / e : 0.f;
-    }
-    // samples near either end: the envelope of the frames that exist
-    auto edgeInv = [&](int64_t p) {
-        float e = 0.f;
-        const int64_t fh = p / hop;
-        for (int64_t f = fh - K + 1 > 0 ? fh - K + 1 : 0; f <= fh && f < (int64_t)frames; ++f) {
-            const int64_t j = p - f * hop;
-            if (j < N) {
-                const float w = window ? __ldg(window + j) : 1.f;
-                e += w * w;
-            }
-        }
-        return e > 0.f ? 1.f / e : 0.f;
-    };
-    // each thread sums VEC consecutive samples: q += VEC*CTA, tracked as (q / hop, q % hop)
-    const int stepH = VEC * CTA / (int)hop, stepR = VEC * CTA - stepH * (int)hop;
-    const int qh0 = VEC * (int)threadIdx.x / (int)hop, qr0 = VEC * (int)threadIdx.x - qh0 * (int)hop;
-    auto clampq = [](int64_t v, int hi) { return (int)(v < 0 ? 0 : (v > hi ? hi : v)); };
+    auto row = [&](int r) { return reinterpret_cast<const float*>(smem + r * S); };
 
-    for (uint32_t f0 = fA; f0 < fB; f0 += ROWS) {
-        const int R = (int)min((uint32_t)ROWS, fB - f0);
+    for (uint32_t f0 = seg.fA; f0 < seg.fB; f0 += ROWS) {
+        const int R = (int)min((uint32_t)ROWS, seg.fB - f0);
         // rows past R (a CTA's partial first or last wave) transform frame f0 again and are not
         // read: every row runs the same barriers, rows of one warp included
         const float2* src = src0 + (uint64_t)(f0 + (rl < R ? rl : 0)) * (M + 1);
@@ -183,85 +134,10 @@ k_istft(const float2* __restrict__ spec, float* __restrict__ out, const float2* 
             sm[i] = make_float2(z.x * w.x, z.y * w.y);
         });
         __syncthreads();
-        const bool tail = f0 + R == frames;   // no later frame: every sample of the span is complete
-        const int span = (R - 1) * (int)hop + N;
-        const int done = tail ? span : R * (int)hop;
-        const int64_t base = (int64_t)f0 * hop;
-        // span offsets q this CTA stores ([wlo, whi)) and those with the periodic envelope
-        const int wlo = clampq((P0 > start ? P0 : start) - base, done);
-        const int whi = clampq((P1 < end ? P1 : end) - base, done);
-        const int elo = clampq((int64_t)(N - 1) - base, span);
-        const int ehi = clampq((int64_t)frames * hop - base, span);
-        float* dq = dst + (base - start);   // output of span offset q at dq[q] (wlo <= q < whi)
-        int qh = qh0, qr = qr0;
-        if constexpr (VEC == 1) {
-            for (int q = threadIdx.x; q < span; q += CTA) {
-                float val = q < CARRY ? cur[q] : 0.f;
-                const int rlo = qh - K + 1 > 0 ? qh - K + 1 : 0;
-                const int rhi = qh < R - 1 ? qh : R - 1;
-                for (int r = rlo; r <= rhi; ++r) {
-                    const int j = qr + (qh - r) * (int)hop;
-                    if (j < N) val += reinterpret_cast<const float*>(smem + r * S)[j];
-                }
-                if (q >= done) {
-                    nxt[q - done] = val;
-                } else if (q >= wlo && q < whi) {
-                    __stcs(dq + q, val * (q >= elo && q < ehi ? rinv[qr] : edgeInv(base + q)));
-                }
-                qh += stepH;
-                qr += stepR;
-                if (qr >= (int)hop) {
-                    qr -= (int)hop;
-                    ++qh;
-                }
-            }
-        } else {
-            // hop, N, CARRY, done, wlo and whi are multiples of 4 and the 4 samples share q / hop:
-            // every shared and global access below is one aligned float4
-            for (int q = 4 * threadIdx.x; q < span; q += 4 * CTA) {
-                float4 val = q < CARRY ? *reinterpret_cast<const float4*>(cur + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-                const int rlo = qh - K + 1 > 0 ? qh - K + 1 : 0;
-                const int rhi = qh < R - 1 ? qh : R - 1;
-                for (int r = rlo; r <= rhi; ++r) {
-                    const int j = qr + (qh - r) * (int)hop;
-                    if (j < N) {
-                        const float4 x = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(smem + r * S) + j);
-                        val.x += x.x;
-                        val.y += x.y;
-                        val.z += x.z;
-                        val.w += x.w;
-                    }
-                }
-                if (q >= done) {
-                    *reinterpret_cast<float4*>(nxt + q - done) = val;
-                } else if (q >= wlo && q < whi) {
-                    float4 e;
-                    if (q >= elo && q + 3 < ehi) {
-                        e = *reinterpret_cast<const float4*>(rinv + qr);
-                    } else {
-                        auto inv = [&](int u) { return q + u >= elo && q + u < ehi ? rinv[qr + u] : edgeInv(base + q + u); };
-                        e = make_float4(inv(0), inv(1), inv(2), inv(3));
-                    }
-                    __stcs(reinterpret_cast<float4*>(dq + q), make_float4(val.x * e.x, val.y * e.y, val.z * e.z, val.w * e.w));
-                }
-                qh += stepH;
-                qr += stepR;
-                if (qr >= (int)hop) {
-                    qr -= (int)hop;
-                    ++qh;
-                }
-            }
-        }
-        float* sw = cur;
-        cur = nxt;
-        nxt = sw;
+        seg.wave<VEC, CTA>(f0, R, [&](int r, int j) { return row(r)[j]; },
+                      [&](int r, int j) { return *reinterpret_cast<const float4*>(row(r) + j); });
     }
-    if (c + 1 == segs) {   // samples past the last frame up to outLen are zero
-        for (int64_t p = (padded > P0 ? padded : P0) + threadIdx.x; p < P1; p += CTA) {
-            const int64_t i = p - start;
-            if (i >= 0 && i < (int64_t)outLen) __stcs(dst + i, 0.f);
-        }
-    }
+    seg.zeroTail(segs);
 }
 
 }  // namespace dev

@@ -758,6 +758,7 @@ int Plan::execStft(const void* dSig, void* dOut, uint32_t n, uint64_t signals, u
                    uint32_t hop, bool center, const void* dWindow, uint64_t* framesOut, void* stream) {
     const bool mixedN = !pow2(n) && realMixed(n);
     if (!impl_ || !dSig || !dOut || signals == 0 || hop == 0 || !(backend::hasStft(n) || mixedN)) return -8;
+    if (reinterpret_cast<uintptr_t>(dWindow) & 7u) return -8;   // the kernels read the window as float2
     if (center ? sigLen <= n / 2 : sigLen < n) return -8;
     const uint64_t frames = center ? 1 + sigLen / hop : 1 + (sigLen - n) / hop;
     if (frames > 0xFFFFFFFFull || signals > (~0ull) / frames) return -8;
@@ -784,6 +785,7 @@ int Plan::execIstft(const void* dSpec, void* dOut, uint32_t n, uint64_t signals,
         !(backend::hasStft(n) || mixedN))
         return -8;
     if (signals * frames > 0xFFFFFFFFull || outLen == 0 || outLen > (1ull << 62)) return -8;
+    if (reinterpret_cast<uintptr_t>(dWindow) & 7u) return -8;   // the kernels read the window as float2
     if (mixedN) {
         if (prepareMixed(n / 2) || prepareReal(n)) return -2;
         const auto& m = impl_->mixed[n / 2];

@@ -160,7 +160,7 @@ int bfly_plan_exec_c2c_axis_async(bfly_plan* plan, const void* d_in, void* d_out
                                   void* stream);
 /* New: STFT of `signals` contiguous fp32 signals of sig_len samples: frames of n samples (n a
  * power of two in [64, 8192], or even with n/2 13-smooth up to 24576) every `hop`, centred with reflect padding when center != 0
- * (sig_len > n/2; torch.stft's defaults), times d_window (n floats, or NULL), one-sided
+ * (sig_len > n/2; torch.stft's defaults), times d_window (n floats, 8-byte aligned, or NULL), one-sided
  * spectrum of every frame into d_out = [signals][frames][n/2+1] complex;
  * frames = center ? 1 + sig_len/hop : 1 + (sig_len-n)/hop, returned in *frames (may be NULL).
  * The reference measures STFT only as a dense-frame R2C proxy (docs/testing.md:118,
@@ -171,7 +171,7 @@ int bfly_plan_exec_stft_async(bfly_plan* plan, const void* d_sig, void* d_out, u
 /* New: inverse STFT (torch.istft), n a power of two in [64, 8192] or even with n/2 13-smooth up
  * to 8192: d_spec = [signals][frames][n/2+1] complex64 -> d_out =
  * [signals][out_len] fp32: every frame inverse-transformed (1/n), then overlap-added with the
- * window (d_window, n floats, or NULL) and divided by the overlap-added squared window, from
+ * window (d_window, n floats, 8-byte aligned, or NULL) and divided by the overlap-added squared window, from
  * padded position n/2 when center != 0, times scale; hop <= n; samples whose window envelope
  * is zero are written as 0.  The reference has no STFT of its own. */
 int bfly_plan_exec_istft_async(bfly_plan* plan, const void* d_spec, void* d_out, uint32_t n,

@@ -492,6 +492,7 @@ int main(int argc, char** argv) {
         CHECK(plan->execStft(d, d, 64, 0, 200, 16, true, nullptr, &fr, nullptr) == -8);     // no signals
         CHECK(plan->execStft(d, d, 64, 1, 32, 16, true, nullptr, &fr, nullptr) == -8);      // reflect needs len > n/2
         CHECK(plan->execStft(d, d, 64, 1, 63, 16, false, nullptr, &fr, nullptr) == -8);     // shorter than a frame
+        CHECK(plan->execStft(d, d, 64, 1, 200, 16, true, d + 1, &fr, nullptr) == -8);       // window not 8-byte aligned
         CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
     }
 
