@@ -4,12 +4,14 @@
 // allocations / copies / launches, and failure injection proving a failed prepare never leaves
 // a stale key.  Adds the B200 runtime's own contracts: host round-trip error codes, measure and
 // select acceptance, and the persisted tuning cache.
+#include "backend.h"
 #include "bfly/plan.hpp"
 
 #include <algorithm>
 #include <cassert>
 #include <cmath>
 #include <cstdio>
+#include <initializer_list>
 #include <cstring>
 #include <fstream>
 #include <functional>
@@ -494,6 +496,39 @@ int main(int argc, char** argv) {
         CHECK(plan->execStft(d, d, 64, 1, 63, 16, false, nullptr, &fr, nullptr) == -8);     // shorter than a frame
         CHECK(plan->execStft(d, d, 64, 1, 200, 16, true, d + 1, &fr, nullptr) == -8);       // window not 8-byte aligned
         CHECK(fake::allocations == allocBefore && fake::launches == launchBefore);
+    }
+
+    {   // mixed-radix planner: every 13-smooth n up to kMixedMaxN (and no other) gets a plan of
+        // radices the kernel implements whose product is n, with consistent Ns and twiddle offsets
+        int plans = 0, maxPasses = 0;
+        for (uint32_t n = 2; n <= bfly::backend::kMixedMaxN; ++n) {
+            uint32_t r = n;
+            for (uint32_t p : {2u, 3u, 5u, 7u, 11u, 13u})
+                while (r % p == 0) r /= p;
+            bfly::backend::MixedRadix m;
+            const bool ok = bfly::backend::mixedRadix(n, &m);
+            CHECK(ok == (r == 1));
+            if (!ok) continue;
+            ++plans;
+            maxPasses = std::max(maxPasses, m.passes);
+            uint64_t prod = 1;
+            int tw = 0;
+            for (int q = 0; q < m.passes; ++q) {
+                const int R = m.radix[q];
+                CHECK(R == 2 || R == 3 || R == 4 || R == 5 || R == 6 || R == 7 || R == 8 || R == 9 || R == 10 ||
+                      R == 11 || R == 12 || R == 13 || R == 14 || R == 15 || R == 16);
+                CHECK(m.ns[q] == (int)prod && m.twoff[q] == tw);
+                if (q) tw += (R - 1) * m.ns[q];
+                prod *= (uint64_t)R;
+            }
+            CHECK(prod == n && m.twsize == tw && m.n == (int)n);
+        }
+        CHECK(plans == 799 && maxPasses <= 5);
+        bfly::backend::MixedRadix m;
+        CHECK(bfly::backend::mixedRadix(1000, &m) && m.passes == 3 && m.radix[0] == 10);      // 10^3
+        CHECK(bfly::backend::mixedRadix(10000, &m) && m.passes == 4);                           // 10^4, not 16 5^4
+        CHECK(bfly::backend::mixedRadix(6561, &m) && m.passes == 4 && m.radix[0] == 9);        // 9^4
+        CHECK(!bfly::backend::mixedRadix(12348, nullptr) && !bfly::backend::mixedRadix(17, nullptr));
     }
 
     {   // real transforms of even non-power-of-two n (n/2 13-smooth): R2C matches a direct DFT,
