@@ -28,38 +28,38 @@ struct MixedArgs {
     int ns[backend::kMixedMaxPasses];
     int twoff[backend::kMixedMaxPasses];
     unsigned magic[backend::kMixedMaxPasses];   // ceil(2^32 / ns), pass p >= 1
-    int pad0;          // the buffer pass 0 writes: element i at i + i / pad0 (pad0 = 0: at i)
-    unsigned magic0;   // ceil(2^32 / pad0)
+    // the buffer pass 0 writes: element i at i + i / pad0, pad0 = R_0 when R_0 is even (its
+    // stride-R_0 stores then hit distinct banks), else 0 (element i at i); the other buffers
+    // hold element i at spad(i)
+    int pad0;
+    unsigned magic0;   // ceil(2^32 / pad0), 0 when pad0 = 0
 };
-
-// Shared-memory position of element i: the buffer pass 0 writes is padded by one slot every
-// pad0 elements (pad0 = R_0 when even, so its stride-R_0 stores hit distinct banks); the
-// others use spad.
-template <bool PASS0_BUF>
-__device__ __forceinline__ int mixed_at(int i, int pad0, unsigned magic0) {
-    if constexpr (PASS0_BUF) return pad0 ? i + (int)__umulhi((unsigned)i, magic0) : i;
-    else return spad(i);
-}
 
 // KIND bit 0: source is the row in HBM (pass 0, which writes the pass-0 buffer); bit 1:
 // destination is the row in HBM (scaled); bit 2: source is the pass-0 buffer (pass 1); bit 3:
 // source is a row staged unpadded in shared memory (pass 0); bit 4: destination is shared
 // memory, unpadded, in natural order (the last pass, for an epilogue).  Pass 0 (Ns = 1) has no
-// twiddles.
+// twiddles.  The pass-0 buffer holds element i at i + i / pad0 (pad0 = R_0 or 0), computed once
+// per butterfly: pass 0 stores j R_0 + r at j (R_0 + 1) + r, and pass 1 reads j + r nb (nb =
+// n / R_1, a multiple of R_0) at j + j / R_0 + r (nb + nb / R_0).
 template <int R, bool INV, int KIND>
 __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float2* __restrict__ dst, int n, int Ns,
                                            unsigned magic, const float2* __restrict__ twp, int t, int T,
                                            float scale, int pad0, unsigned magic0) {
     constexpr bool PASS0 = (KIND & 9) != 0;
     const int nb = n / R;
+    const int nbs = (KIND & 4) ? nb + (int)__umulhi((unsigned)nb, magic0) : nb;
+    const int stride0 = pad0 ? R + 1 : R;
     for (int j = t; j < nb; j += T) {
         const int k = PASS0 ? 0 : j - Ns * (int)__umulhi((unsigned)j, magic);
+        const int js = (KIND & 4) ? j + (int)__umulhi((unsigned)j, magic0) : j;
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r)
             v[r] = (KIND & 1)   ? ld_stream(src + j + r * nb)
                    : (KIND & 8) ? src[j + r * nb]
-                                : src[mixed_at<(KIND & 4) != 0>(j + r * nb, pad0, magic0)];
+                   : (KIND & 4) ? src[js + r * nbs]
+                                : src[spad(j + r * nb)];
         if (!PASS0) {
 #pragma unroll
             for (int r = 1; r < R; ++r) v[r] = cmul<INV>(v[r], __ldg(twp + (r - 1) * Ns + k));
@@ -70,46 +70,48 @@ __device__ __forceinline__ void mixed_pass(const float2* __restrict__ src, float
         for (int r = 0; r < R; ++r) {
             if (KIND & 2) st_stream(dst + base + r * Ns, cscale(v[r], scale));
             else if (KIND & 16) dst[base + r * Ns] = v[r];
-            else dst[mixed_at<PASS0>(base + r * Ns, pad0, magic0)] = v[r];
+            else if (PASS0) dst[j * stride0 + r] = v[r];
+            else dst[spad(base + r * Ns)] = v[r];
         }
     }
 }
 
-// WIDE adds the prime radices 11 and 13 (their butterflies need more registers, so plans
-// without them run an instance compiled without those cases).
-template <bool INV, int KIND, bool WIDE>
+// Radix classes: CLS 0 compiles the radices up to 10, CLS 1 adds 12, 14, 15 and 16, CLS 2 the
+// primes 11 and 13 (larger butterflies need more registers, and a kernel is allocated for its
+// largest, so each plan runs the smallest class holding its radices).
+template <bool INV, int KIND, int CLS>
 __device__ __forceinline__ void mixed_pass_r(int R, const float2* src, float2* dst, int n, int Ns, unsigned magic,
                                              const float2* twp, int t, int T, float scale, int pad0,
                                              unsigned magic0) {
-    if constexpr (WIDE) {
-        if (R == 13) return mixed_pass<13, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0);
-        if (R == 11) return mixed_pass<11, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0);
-    }
 #define BFLY_MP(RR) \
-    case RR: mixed_pass<RR, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0); break
-    switch (R) {
+    if (R == RR) return mixed_pass<RR, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0)
+    if constexpr (CLS >= 2) {
+        BFLY_MP(13);
+        BFLY_MP(11);
+    }
+    if constexpr (CLS >= 1) {
         BFLY_MP(16);
         BFLY_MP(15);
         BFLY_MP(14);
         BFLY_MP(12);
-        BFLY_MP(10);
-        BFLY_MP(9);
-        BFLY_MP(8);
-        BFLY_MP(7);
-        BFLY_MP(6);
-        BFLY_MP(5);
-        BFLY_MP(4);
-        BFLY_MP(3);
-        default: mixed_pass<2, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0); break;
     }
+    BFLY_MP(10);
+    BFLY_MP(9);
+    BFLY_MP(8);
+    BFLY_MP(7);
+    BFLY_MP(6);
+    BFLY_MP(5);
+    BFLY_MP(4);
+    BFLY_MP(3);
 #undef BFLY_MP
+    mixed_pass<2, INV, KIND>(src, dst, n, Ns, magic, twp, t, T, scale, pad0, magic0);
 }
 
 // The passes of one row.  Pass 0 reads the row from HBM (SRC_HBM) or unpadded from buf1 (a
 // stage written before the call); the last pass writes the row to HBM times `scale` (DST_HBM)
 // or unpadded, natural order, into the buffer returned (buf0 or buf1).  All threads of the CTA
 // call it (rows whose `ok` is false skip the work, not the barriers).
-template <bool INV, bool WIDE, bool SRC_HBM, bool DST_HBM>
+template <bool INV, int CLS, bool SRC_HBM, bool DST_HBM>
 __device__ __forceinline__ float2* mixed_row(const MixedArgs& a, const float2* src, float2* dst, float2* buf0,
                                              float2* buf1, const float2* __restrict__ tw, bool ok, int t, int T,
                                              float scale) {
@@ -128,12 +130,12 @@ __device__ __forceinline__ float2* mixed_row(const MixedArgs& a, const float2* s
         const int p0 = a.pad0;
         const unsigned m0 = a.magic0;
         if (ok) {
-            if (first && last) mixed_pass_r<INV, K0 | KL, WIDE>(R, SRC_HBM ? src : sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (first) mixed_pass_r<INV, K0, WIDE>(R, SRC_HBM ? src : sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (p == 1 && last) mixed_pass_r<INV, 4 | KL, WIDE>(R, sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (p == 1) mixed_pass_r<INV, 4, WIDE>(R, sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else if (last) mixed_pass_r<INV, KL, WIDE>(R, sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
-            else mixed_pass_r<INV, 0, WIDE>(R, sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
+            if (first && last) mixed_pass_r<INV, K0 | KL, CLS>(R, SRC_HBM ? src : sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (first) mixed_pass_r<INV, K0, CLS>(R, SRC_HBM ? src : sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (p == 1 && last) mixed_pass_r<INV, 4 | KL, CLS>(R, sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (p == 1) mixed_pass_r<INV, 4, CLS>(R, sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else if (last) mixed_pass_r<INV, KL, CLS>(R, sb, dl, n, Ns, mg, twp, t, T, scale, p0, m0);
+            else mixed_pass_r<INV, 0, CLS>(R, sb, db, n, Ns, mg, twp, t, T, scale, p0, m0);
         }
         if (last) fin = db;
         if (!last) __syncthreads();
@@ -141,7 +143,7 @@ __device__ __forceinline__ float2* mixed_row(const MixedArgs& a, const float2* s
     return fin;
 }
 
-template <bool INV, bool WIDE>
+template <bool INV, int CLS>
 __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in, float2* __restrict__ out,
                                                   const float2* __restrict__ tw, MixedArgs a, uint64_t batch, int T,
                                                   int rows, int len, float scale) {
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in,
     const uint64_t row = (uint64_t)blockIdx.x * rows + rl;
     const bool ok = rl < rows && row < batch;
     float2* buf0 = smem + (size_t)(rl < rows ? rl : 0) * 2 * len;
-    mixed_row<INV, WIDE, true, true>(a, in + row * a.n, out + row * a.n, buf0, buf0 + len, tw, ok, t, T, scale);
+    mixed_row<INV, CLS, true, true>(a, in + row * a.n, out + row * a.n, buf0, buf0 + len, tw, ok, t, T, scale);
 }
 
 // Real transforms of even length N = 2M on the mixed-radix passes of the M-point complex row
@@ -159,7 +161,7 @@ __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in,
 // R2C (numpy.fft.rfft): z[m] = x[2m] + i x[2m+1] read as complex, Z = FFT_M(z) left unpadded in
 // shared memory, then per bin k <= M: a = Z[k mod M], b = conj(Z[(M-k) mod M]),
 // X[k] = (a+b)/2 + W_N^k (a-b)/(2i), times s_edge at bins 0 and M and s_int elsewhere.
-template <bool WIDE>
+template <int CLS>
 __global__ void __launch_bounds__(512, 2) k_r2c_mixed(const float2* __restrict__ in, float2* __restrict__ out,
                                                       const float2* __restrict__ tw, const float2* __restrict__ twr,
                                                       MixedArgs a, uint64_t batch, int T, int rows, int len,
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(512, 2) k_r2c_mixed(const float2* __restrict__
     const bool ok = rl < rows && row < batch;
     const int M = a.n;
     float2* buf0 = smem + (size_t)(rl < rows ? rl : 0) * 2 * len;
-    const float2* Z = mixed_row<false, WIDE, true, false>(a, in + row * M, nullptr, buf0, buf0 + len, tw, ok, t, T,
+    const float2* Z = mixed_row<false, CLS, true, false>(a, in + row * M, nullptr, buf0, buf0 + len, tw, ok, t, T,
                                                            1.f);
     __syncthreads();
     if (!ok) return;
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(512, 2) k_r2c_mixed(const float2* __restrict__
 // Z[k] = (Xk + conj Xm) + i (Xk - conj Xm) W_N^-k (Xm = X[M-k], X[M] for k = 0; imaginary parts of
 // bins 0 and M ignored; s_edge / s_int per bin; out_scale) is staged unpadded in shared memory,
 // then z = IFFT_M(Z) goes to HBM as x[2m] = Re z[m], x[2m+1] = Im z[m].
-template <bool WIDE>
+template <int CLS>
 __global__ void __launch_bounds__(512, 2) k_c2r_mixed(const float2* __restrict__ in, float2* __restrict__ out,
                                                       const float2* __restrict__ tw, const float2* __restrict__ twr,
                                                       MixedArgs a, uint64_t batch, int T, int rows, int len,
@@ -209,12 +211,12 @@ __global__ void __launch_bounds__(512, 2) k_c2r_mixed(const float2* __restrict__
             buf1[k] = c2r_split(ld_stream(src + k), ld_stream(src + (k == 0 ? M : M - k)), k, __ldg(twr + k), s_edge,
                                 s_int, out_scale);
     __syncthreads();
-    mixed_row<true, WIDE, false, true>(a, nullptr, out + row * M, buf0, buf1, tw, ok, t, T, 1.f);
+    mixed_row<true, CLS, false, true>(a, nullptr, out + row * M, buf0, buf1, tw, ok, t, T, 1.f);
 }
 
 // STFT: frame f of signal s, y[j] = w[j] x_s[f hop + j - (center ? N/2 : 0)] (reflect padding,
 // as k_stft), packed as z[m] = y[2m] + i y[2m+1] and staged unpadded; then the R2C of k_r2c_mixed.
-template <bool WIDE>
+template <int CLS>
 __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__ sig, float2* __restrict__ out,
                                                        const float2* __restrict__ tw, const float2* __restrict__ twr,
                                                        const float* __restrict__ window, MixedArgs a, uint64_t frames,
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__
         }
     }
     __syncthreads();
-    const float2* Z = mixed_row<false, WIDE, false, false>(a, nullptr, nullptr, buf0, buf1, tw, ok, t, T, 1.f);
+    const float2* Z = mixed_row<false, CLS, false, false>(a, nullptr, nullptr, buf0, buf1, tw, ok, t, T, 1.f);
     __syncthreads();
     if (!ok) return;
     float2* dst = out + row * (uint64_t)(M + 1);
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__
 // stages its frame's un-split spectrum (c2r_split, out_scale) in buf1 and runs the M-point
 // inverse passes into its natural-order row buffer; the segment split, carry, envelope and
 // overlap-add (window applied there) are IstftSegment (istft_ola.cuh), as in k_istft.
-template <bool WIDE, int VEC>
+template <int CLS, int VEC>
 __global__ void __launch_bounds__(512, 2) k_istft_mixed(const float2* __restrict__ spec, float* __restrict__ out,
                                                         const float2* __restrict__ tw, const float2* __restrict__ twr,
                                                         const float* __restrict__ window, MixedArgs a, uint32_t frames,
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(512, 2) k_istft_mixed(const float2* __restrict
             buf1[k] = c2r_split(ld_stream(src + k), ld_stream(src + (k == 0 ? M : M - k)), k, __ldg(twr + k), 1.f, 1.f,
                                 out_scale);
         __syncthreads();
-        mixed_row<true, WIDE, false, false>(a, nullptr, nullptr, buf0, buf1, tw, true, t, T, 1.f);
+        mixed_row<true, CLS, false, false>(a, nullptr, nullptr, buf0, buf1, tw, true, t, T, 1.f);
         __syncthreads();
         seg.wave<VEC, 0>(
             f0, R, [&](int r, int j) { return (window ? __ldg(window + j) : 1.f) * frameOf(r)[j]; },
@@ -360,10 +362,10 @@ namespace {
 struct MixedShape {
     dev::MixedArgs args;
     int T = 0, rows = 0, len = 0, smem = 0;
-    bool wide = false;
+    int cls = 0;   // radix class of the kernel instance (mixed_pass_r)
 };
-constexpr int kMixedMaxSmem = 2 * (dev::spad((int)kMixedMaxN - 1) + 1) * 8;
-static_assert(kMixedMaxSmem <= 227 * 1024, "two rows of the longest length fit in shared memory");
+constexpr int kMixedMaxSmem = 227 * 1024;
+static_assert(2 * (dev::spad((int)kMixedMaxN - 1) + 1) * 8 <= kMixedMaxSmem, "two rows of the longest length fit in shared memory");
 
 MixedShape mixedShape(const MixedRadix& plan) {
     MixedShape m;
@@ -374,24 +376,29 @@ MixedShape mixedShape(const MixedRadix& plan) {
     int rmax = 2;
     for (int p = 0; p < plan.passes; ++p) {
         rmax = std::max(rmax, plan.radix[p]);
-        m.wide = m.wide || plan.radix[p] == 11 || plan.radix[p] == 13;
+        m.cls = std::max(m.cls, plan.radix[p] == 11 || plan.radix[p] == 13 ? 2 : plan.radix[p] > 10 ? 1 : 0);
     }
     m.T = std::min(512, (plan.n + rmax - 1) / rmax);
     m.rows = std::max(1, 224 / m.T);
     // pass 0 stores at stride R_0: pad its buffer every R_0 slots when R_0 is even (odd strides
-    // are conflict-free already), unless that no longer fits; pad 16 is spad's layout
+    // are conflict-free already), unless that no longer fits (then it stays unpadded)
     const int r0 = plan.radix[0];
     m.len = dev::spad(plan.n - 1) + 1;
     m.args.pad0 = (r0 % 2 == 0 && plan.passes > 1) ? r0 : 0;
     if (m.args.pad0) {
         const int len0 = std::max(m.len, plan.n + (plan.n - 1) / m.args.pad0 + 1);
         if (m.rows * 2 * len0 * 8 <= kMixedMaxSmem) m.len = len0;
-        else m.args.pad0 = 16;
+        else m.args.pad0 = 0;
     }
     m.args.magic0 =
         m.args.pad0 ? (unsigned)((0x100000000ull + m.args.pad0 - 1) / (unsigned long long)m.args.pad0) : 0u;
     m.smem = m.rows * 2 * m.len * 8;
     return m;
+}
+
+template <class F>
+F* byClass(int cls, F* c0, F* c1, F* c2) {
+    return cls == 0 ? c0 : cls == 1 ? c1 : c2;
 }
 }  // namespace
 
@@ -399,9 +406,9 @@ int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batc
                 const void* tw, void* stream) {
     if (!mixedValid(plan)) return (int)cudaErrorInvalidValue;
     const MixedShape m = mixedShape(plan);
-    auto* fn = inverse ? (m.wide ? dev::k_mixed<true, true> : dev::k_mixed<true, false>)
-                       : (m.wide ? dev::k_mixed<false, true> : dev::k_mixed<false, false>);
-    // opted in once per device at kMixedMaxSmem (the largest row pair: n = kMixedMaxN, one row per CTA)
+    auto* fn = inverse ? byClass(m.cls, dev::k_mixed<true, 0>, dev::k_mixed<true, 1>, dev::k_mixed<true, 2>)
+                       : byClass(m.cls, dev::k_mixed<false, 0>, dev::k_mixed<false, 1>, dev::k_mixed<false, 2>);
+    // opted in once per device at kMixedMaxSmem
     if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
     const uint64_t groups = (batch + m.rows - 1) / m.rows;
@@ -416,7 +423,7 @@ int launchR2CMixed(const void* in, void* out, const MixedRadix& half, uint64_t b
                    float sEdge, float sInt, void* stream) {
     if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
     const MixedShape m = mixedShape(half);
-    auto* fn = m.wide ? dev::k_r2c_mixed<true> : dev::k_r2c_mixed<false>;
+    auto* fn = byClass(m.cls, dev::k_r2c_mixed<0>, dev::k_r2c_mixed<1>, dev::k_r2c_mixed<2>);
     if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
     const uint64_t groups = (batch + m.rows - 1) / m.rows;
@@ -431,7 +438,7 @@ int launchC2RMixed(const void* in, void* out, const MixedRadix& half, uint64_t b
                    float sEdge, float sInt, float outScale, void* stream) {
     if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
     const MixedShape m = mixedShape(half);
-    auto* fn = m.wide ? dev::k_c2r_mixed<true> : dev::k_c2r_mixed<false>;
+    auto* fn = byClass(m.cls, dev::k_c2r_mixed<0>, dev::k_c2r_mixed<1>, dev::k_c2r_mixed<2>);
     if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
     const uint64_t groups = (batch + m.rows - 1) / m.rows;
@@ -447,7 +454,7 @@ int launchStftMixed(const void* sig, void* out, const MixedRadix& half, uint64_t
                     const void* tw, const void* twr, void* stream) {
     if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
     const MixedShape m = mixedShape(half);
-    auto* fn = m.wide ? dev::k_stft_mixed<true> : dev::k_stft_mixed<false>;
+    auto* fn = byClass(m.cls, dev::k_stft_mixed<0>, dev::k_stft_mixed<1>, dev::k_stft_mixed<2>);
     if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
     const uint64_t frames = signals * framesPerSignal;
@@ -477,8 +484,8 @@ int launchIstftMixed(const void* spec, void* out, const MixedRadix& half, uint64
     // and window (a frame of N % 4 == 2 would read past its row)
     const bool vec = N % 4 == 0 && hop % 4 == 0 && outLen % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15u) == 0 &&
                      (reinterpret_cast<uintptr_t>(window) & 15u) == 0;
-    auto* fn = m.wide ? (vec ? dev::k_istft_mixed<true, 4> : dev::k_istft_mixed<true, 1>)
-                      : (vec ? dev::k_istft_mixed<false, 4> : dev::k_istft_mixed<false, 1>);
+    auto* fn = vec ? byClass(m.cls, dev::k_istft_mixed<0, 4>, dev::k_istft_mixed<1, 4>, dev::k_istft_mixed<2, 4>)
+                   : byClass(m.cls, dev::k_istft_mixed<0, 1>, dev::k_istft_mixed<1, 1>, dev::k_istft_mixed<2, 1>);
     if (int e = optInSharedMemory((const void*)fn, kMaxSmem)) return e;
     int device = 0, sms = 0, perSm = 0;
     if (cudaGetDevice(&device) != cudaSuccess ||
