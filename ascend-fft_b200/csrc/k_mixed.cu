@@ -9,10 +9,14 @@
 // there, so the store index is j + r n/R, coalesced too).  T = min(512, ceil(n / R_max)) threads
 // per row, each taking butterflies j = t, t + T, ...; max(1, 224 / T) rows per CTA.  k = j mod Ns
 // uses a multiply-high by ceil(2^32 / Ns) (exact for j, Ns < 2^14).  The pass list is a kernel
-// argument, so one kernel serves every such length.
+// argument, so one kernel (per radix class) serves every such length; the plans of common
+// lengths also have kernels with the pass list fixed at compile time (FixedRows), whose
+// constant offsets and strides take a third to a half of the instructions off each pass.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <initializer_list>
+#include <tuple>
 
 #include "backend.h"
 #include "fft_kernels.cuh"
@@ -143,7 +147,98 @@ __device__ __forceinline__ float2* mixed_row(const MixedArgs& a, const float2* s
     return fin;
 }
 
-template <bool INV, int CLS>
+// The same passes for a plan fixed at compile time (its radices R0, R1, ...): n, Ns, the
+// butterfly counts, threads per row and the pass-0 pad are constants, so the element offsets
+// of every load and store fold into the instructions and the radix needs no dispatch.  T =
+// min(512, ceil(n / R_max)) threads per row and pad0 = R_0 (even R_0) or 0, as mixedShape
+// sets them; twiddles at the plan's offsets.
+template <int R, bool INV, int KIND, int N, int NS, int T, int PAD0>
+__device__ __forceinline__ void fixed_pass(const float2* __restrict__ src, float2* __restrict__ dst,
+                                           const float2* __restrict__ twp, int t, float scale) {
+    constexpr bool PASS0 = (KIND & 9) != 0;
+    constexpr int nb = N / R;
+    constexpr int nbs = (KIND & 4) && PAD0 ? nb + nb / PAD0 : nb;
+    constexpr int stride0 = PAD0 ? R + 1 : R;
+#pragma unroll
+    for (int j0 = 0; j0 < nb; j0 += T) {
+        const int j = j0 + t;
+        if (nb % T != 0 && j >= nb) break;
+        const int k = PASS0 ? 0 : j % NS;
+        const int js = (KIND & 4) && PAD0 ? j + j / PAD0 : j;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            v[r] = (KIND & 1)   ? ld_stream(src + j + r * nb)
+                   : (KIND & 8) ? src[j + r * nb]
+                   : (KIND & 4) ? src[js + r * nbs]
+                                : src[spad(j + r * nb)];
+        if (!PASS0) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul<INV>(v[r], __ldg(twp + (r - 1) * NS + k));
+        }
+        DFT<R, INV>::run(v);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (KIND & 2) st_stream(dst + base + r * NS, cscale(v[r], scale));
+            else if (KIND & 16) dst[base + r * NS] = v[r];
+            else if (PASS0) dst[j * stride0 + r] = v[r];
+            else dst[spad(base + r * NS)] = v[r];
+        }
+    }
+}
+
+template <int... Rs>
+struct FixedPlan {
+    static constexpr int N = (Rs * ...);
+    static constexpr int RMAX = std::max({Rs...});
+    static constexpr int T = (N + RMAX - 1) / RMAX < 512 ? (N + RMAX - 1) / RMAX : 512;
+    static constexpr int R0 = std::get<0>(std::make_tuple(Rs...));
+    static constexpr int PAD0 = (R0 % 2 == 0 && sizeof...(Rs) > 1) ? R0 : 0;
+};
+
+template <bool INV, class FP, bool SRC_HBM, bool DST_HBM, int P, int NS, int R, int... Rest>
+__device__ __forceinline__ float2* fixed_row(const float2* src, float2* dst, float2* buf0, float2* buf1,
+                                             const float2* __restrict__ tw, const int* twoff, bool ok, int t,
+                                             float scale) {
+    constexpr bool LAST = sizeof...(Rest) == 0;
+    constexpr int KIND = (P == 0 ? (SRC_HBM ? 1 : 8) : (P == 1 ? 4 : 0)) | (LAST ? (DST_HBM ? 2 : 16) : 0);
+    const float2* sb = (P & 1) ? buf0 : buf1;
+    float2* db = (P & 1) ? buf1 : buf0;
+    if (ok)
+        fixed_pass<R, INV, KIND, FP::N, NS, FP::T, FP::PAD0>(P == 0 && SRC_HBM ? src : sb, LAST && DST_HBM ? dst : db,
+                                                            tw + twoff[P], t, scale);
+    if constexpr (LAST) {
+        return db;
+    } else {
+        __syncthreads();
+        return fixed_row<INV, FP, SRC_HBM, DST_HBM, P + 1, NS * R, Rest...>(src, dst, buf0, buf1, tw, twoff, ok, t, scale);
+    }
+}
+
+// Row policies of the kernels below: the runtime pass list (radix class CLS) or a plan fixed at
+// compile time (Rs; launched with its T and pad0 only).
+template <int CLS>
+struct GenericRows {
+    template <bool INV, bool SRC_HBM, bool DST_HBM>
+    static __device__ __forceinline__ float2* run(const MixedArgs& a, const float2* src, float2* dst, float2* buf0,
+                                                  float2* buf1, const float2* __restrict__ tw, bool ok, int t, int T,
+                                                  float scale) {
+        return mixed_row<INV, CLS, SRC_HBM, DST_HBM>(a, src, dst, buf0, buf1, tw, ok, t, T, scale);
+    }
+};
+template <int... Rs>
+struct FixedRows {
+    template <bool INV, bool SRC_HBM, bool DST_HBM>
+    static __device__ __forceinline__ float2* run(const MixedArgs& a, const float2* src, float2* dst, float2* buf0,
+                                                  float2* buf1, const float2* __restrict__ tw, bool ok, int t, int,
+                                                  float scale) {
+        return fixed_row<INV, FixedPlan<Rs...>, SRC_HBM, DST_HBM, 0, 1, Rs...>(src, dst, buf0, buf1, tw, a.twoff, ok, t,
+                                                                             scale);
+    }
+};
+
+template <bool INV, class ROWS>
 __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in, float2* __restrict__ out,
                                                   const float2* __restrict__ tw, MixedArgs a, uint64_t batch, int T,
                                                   int rows, int len, float scale) {
@@ -153,7 +248,7 @@ __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in,
     const uint64_t row = (uint64_t)blockIdx.x * rows + rl;
     const bool ok = rl < rows && row < batch;
     float2* buf0 = smem + (size_t)(rl < rows ? rl : 0) * 2 * len;
-    mixed_row<INV, CLS, true, true>(a, in + row * a.n, out + row * a.n, buf0, buf0 + len, tw, ok, t, T, scale);
+    ROWS::template run<INV, true, true>(a, in + row * a.n, out + row * a.n, buf0, buf0 + len, tw, ok, t, T, scale);
 }
 
 // Real transforms of even length N = 2M on the mixed-radix passes of the M-point complex row
@@ -161,7 +256,7 @@ __global__ void __launch_bounds__(512, 2) k_mixed(const float2* __restrict__ in,
 // R2C (numpy.fft.rfft): z[m] = x[2m] + i x[2m+1] read as complex, Z = FFT_M(z) left unpadded in
 // shared memory, then per bin k <= M: a = Z[k mod M], b = conj(Z[(M-k) mod M]),
 // X[k] = (a+b)/2 + W_N^k (a-b)/(2i), times s_edge at bins 0 and M and s_int elsewhere.
-template <int CLS>
+template <class ROWS>
 __global__ void __launch_bounds__(512, 2) k_r2c_mixed(const float2* __restrict__ in, float2* __restrict__ out,
                                                       const float2* __restrict__ tw, const float2* __restrict__ twr,
                                                       MixedArgs a, uint64_t batch, int T, int rows, int len,
@@ -173,7 +268,7 @@ __global__ void __launch_bounds__(512, 2) k_r2c_mixed(const float2* __restrict__
     const bool ok = rl < rows && row < batch;
     const int M = a.n;
     float2* buf0 = smem + (size_t)(rl < rows ? rl : 0) * 2 * len;
-    const float2* Z = mixed_row<false, CLS, true, false>(a, in + row * M, nullptr, buf0, buf0 + len, tw, ok, t, T,
+    const float2* Z = ROWS::template run<false, true, false>(a, in + row * M, nullptr, buf0, buf0 + len, tw, ok, t, T,
                                                            1.f);
     __syncthreads();
     if (!ok) return;
@@ -192,7 +287,7 @@ __global__ void __launch_bounds__(512, 2) k_r2c_mixed(const float2* __restrict__
 // Z[k] = (Xk + conj Xm) + i (Xk - conj Xm) W_N^-k (Xm = X[M-k], X[M] for k = 0; imaginary parts of
 // bins 0 and M ignored; s_edge / s_int per bin; out_scale) is staged unpadded in shared memory,
 // then z = IFFT_M(Z) goes to HBM as x[2m] = Re z[m], x[2m+1] = Im z[m].
-template <int CLS>
+template <class ROWS>
 __global__ void __launch_bounds__(512, 2) k_c2r_mixed(const float2* __restrict__ in, float2* __restrict__ out,
                                                       const float2* __restrict__ tw, const float2* __restrict__ twr,
                                                       MixedArgs a, uint64_t batch, int T, int rows, int len,
@@ -211,12 +306,12 @@ __global__ void __launch_bounds__(512, 2) k_c2r_mixed(const float2* __restrict__
             buf1[k] = c2r_split(ld_stream(src + k), ld_stream(src + (k == 0 ? M : M - k)), k, __ldg(twr + k), s_edge,
                                 s_int, out_scale);
     __syncthreads();
-    mixed_row<true, CLS, false, true>(a, nullptr, out + row * M, buf0, buf1, tw, ok, t, T, 1.f);
+    ROWS::template run<true, false, true>(a, nullptr, out + row * M, buf0, buf1, tw, ok, t, T, 1.f);
 }
 
 // STFT: frame f of signal s, y[j] = w[j] x_s[f hop + j - (center ? N/2 : 0)] (reflect padding,
 // as k_stft), packed as z[m] = y[2m] + i y[2m+1] and staged unpadded; then the R2C of k_r2c_mixed.
-template <int CLS>
+template <class ROWS>
 __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__ sig, float2* __restrict__ out,
                                                        const float2* __restrict__ tw, const float2* __restrict__ twr,
                                                        const float* __restrict__ window, MixedArgs a, uint64_t frames,
@@ -254,7 +349,7 @@ __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__
         }
     }
     __syncthreads();
-    const float2* Z = mixed_row<false, CLS, false, false>(a, nullptr, nullptr, buf0, buf1, tw, ok, t, T, 1.f);
+    const float2* Z = ROWS::template run<false, false, false>(a, nullptr, nullptr, buf0, buf1, tw, ok, t, T, 1.f);
     __syncthreads();
     if (!ok) return;
     float2* dst = out + row * (uint64_t)(M + 1);
@@ -271,7 +366,7 @@ __global__ void __launch_bounds__(512, 2) k_stft_mixed(const float* __restrict__
 // stages its frame's un-split spectrum (c2r_split, out_scale) in buf1 and runs the M-point
 // inverse passes into its natural-order row buffer; the segment split, carry, envelope and
 // overlap-add (window applied there) are IstftSegment (istft_ola.cuh), as in k_istft.
-template <int CLS, int VEC>
+template <class ROWS, int VEC>
 __global__ void __launch_bounds__(512, 2) k_istft_mixed(const float2* __restrict__ spec, float* __restrict__ out,
                                                         const float2* __restrict__ tw, const float2* __restrict__ twr,
                                                         const float* __restrict__ window, MixedArgs a, uint32_t frames,
@@ -299,7 +394,7 @@ __global__ void __launch_bounds__(512, 2) k_istft_mixed(const float2* __restrict
             buf1[k] = c2r_split(ld_stream(src + k), ld_stream(src + (k == 0 ? M : M - k)), k, __ldg(twr + k), 1.f, 1.f,
                                 out_scale);
         __syncthreads();
-        mixed_row<true, CLS, false, false>(a, nullptr, nullptr, buf0, buf1, tw, true, t, T, 1.f);
+        ROWS::template run<true, false, false>(a, nullptr, nullptr, buf0, buf1, tw, true, t, T, 1.f);
         __syncthreads();
         seg.wave<VEC, 0>(
             f0, R, [&](int r, int j) { return (window ? __ldg(window + j) : 1.f) * frameOf(r)[j]; },
@@ -396,9 +491,79 @@ MixedShape mixedShape(const MixedRadix& plan) {
     return m;
 }
 
-template <class F>
-F* byClass(int cls, F* c0, F* c1, F* c2) {
-    return cls == 0 ? c0 : cls == 1 ? c1 : c2;
+// The kernels of one row policy.
+using C2CFn = decltype(&dev::k_mixed<false, dev::GenericRows<0>>);
+using R2CFn = decltype(&dev::k_r2c_mixed<dev::GenericRows<0>>);
+using C2RFn = decltype(&dev::k_c2r_mixed<dev::GenericRows<0>>);
+using StftFn = decltype(&dev::k_stft_mixed<dev::GenericRows<0>>);
+using IstftFn = decltype(&dev::k_istft_mixed<dev::GenericRows<0>, 1>);
+struct MixedKernels {
+    C2CFn fwd, inv;
+    R2CFn r2c;
+    C2RFn c2r;
+    StftFn stft;
+    IstftFn istft1, istft4;
+};
+template <class ROWS>
+MixedKernels kernelsOf() {
+    return {dev::k_mixed<false, ROWS>, dev::k_mixed<true, ROWS>, dev::k_r2c_mixed<ROWS>, dev::k_c2r_mixed<ROWS>,
+            dev::k_stft_mixed<ROWS>, dev::k_istft_mixed<ROWS, 1>, dev::k_istft_mixed<ROWS, 4>};
+}
+
+// Plans with compile-time kernels (common lengths: multiples of 10 and the half lengths of the
+// real transforms of n = 400, 480, 1000, 2000, 6000 ...); every other plan runs the runtime
+// pass list of its radix class.
+struct FixedEntry {
+    int passes;
+    int radix[5];
+    int T, pad0;   // the shape the kernels are compiled for
+    MixedKernels k;
+};
+#define BFLY_FIXED(...)                                                                              \
+    {(int)std::initializer_list<int>{__VA_ARGS__}.size(), {__VA_ARGS__}, dev::FixedPlan<__VA_ARGS__>::T, \
+     dev::FixedPlan<__VA_ARGS__>::PAD0, kernelsOf<dev::FixedRows<__VA_ARGS__>>()}
+const FixedEntry kFixed[] = {
+    BFLY_FIXED(10, 10),          // 100
+    BFLY_FIXED(15, 8),           // 120
+    BFLY_FIXED(15, 10),          // 150
+    BFLY_FIXED(16, 10),          // 160
+    BFLY_FIXED(10, 10, 2),       // 200
+    BFLY_FIXED(16, 15),          // 240
+    BFLY_FIXED(10, 5, 5),        // 250
+    BFLY_FIXED(15, 10, 2),       // 300
+    BFLY_FIXED(15, 12, 2),       // 360
+    BFLY_FIXED(16, 5, 5),        // 400
+    BFLY_FIXED(10, 10, 5),       // 500
+    BFLY_FIXED(15, 10, 4),       // 600
+    BFLY_FIXED(15, 10, 5),       // 750
+    BFLY_FIXED(16, 10, 5),       // 800
+    BFLY_FIXED(10, 10, 10),      // 1000
+    BFLY_FIXED(16, 15, 5),       // 1200
+    BFLY_FIXED(15, 10, 10),      // 1500
+    BFLY_FIXED(16, 5, 5, 5),     // 2000
+    BFLY_FIXED(16, 15, 10),      // 2400
+    BFLY_FIXED(10, 10, 5, 5),    // 2500
+    BFLY_FIXED(15, 10, 10, 2),   // 3000
+    BFLY_FIXED(16, 10, 5, 5),    // 4000
+    BFLY_FIXED(10, 10, 10, 5),   // 5000
+    BFLY_FIXED(16, 15, 5, 5),    // 6000
+    BFLY_FIXED(9, 9, 9, 9),      // 6561
+    BFLY_FIXED(16, 10, 10, 5),   // 8000
+    BFLY_FIXED(10, 10, 10, 10),  // 10000
+    BFLY_FIXED(16, 15, 10, 5),   // 12000
+};
+#undef BFLY_FIXED
+
+MixedKernels kernelsFor(const MixedRadix& plan, const MixedShape& m) {
+    for (const FixedEntry& e : kFixed) {
+        if (e.passes != plan.passes || e.T != m.T || e.pad0 != m.args.pad0) continue;
+        bool same = true;
+        for (int p = 0; p < e.passes; ++p) same = same && e.radix[p] == plan.radix[p];
+        if (same) return e.k;
+    }
+    static const MixedKernels generic[3] = {kernelsOf<dev::GenericRows<0>>(), kernelsOf<dev::GenericRows<1>>(),
+                                            kernelsOf<dev::GenericRows<2>>()};
+    return generic[m.cls];
 }
 }  // namespace
 
@@ -406,8 +571,8 @@ int launchMixed(const void* in, void* out, const MixedRadix& plan, uint64_t batc
                 const void* tw, void* stream) {
     if (!mixedValid(plan)) return (int)cudaErrorInvalidValue;
     const MixedShape m = mixedShape(plan);
-    auto* fn = inverse ? byClass(m.cls, dev::k_mixed<true, 0>, dev::k_mixed<true, 1>, dev::k_mixed<true, 2>)
-                       : byClass(m.cls, dev::k_mixed<false, 0>, dev::k_mixed<false, 1>, dev::k_mixed<false, 2>);
+    const MixedKernels k = kernelsFor(plan, m);
+    auto* fn = inverse ? k.inv : k.fwd;
     // opted in once per device at kMixedMaxSmem
     if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
@@ -423,7 +588,7 @@ int launchR2CMixed(const void* in, void* out, const MixedRadix& half, uint64_t b
                    float sEdge, float sInt, void* stream) {
     if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
     const MixedShape m = mixedShape(half);
-    auto* fn = byClass(m.cls, dev::k_r2c_mixed<0>, dev::k_r2c_mixed<1>, dev::k_r2c_mixed<2>);
+    auto* fn = kernelsFor(half, m).r2c;
     if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
     const uint64_t groups = (batch + m.rows - 1) / m.rows;
@@ -438,7 +603,7 @@ int launchC2RMixed(const void* in, void* out, const MixedRadix& half, uint64_t b
                    float sEdge, float sInt, float outScale, void* stream) {
     if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
     const MixedShape m = mixedShape(half);
-    auto* fn = byClass(m.cls, dev::k_c2r_mixed<0>, dev::k_c2r_mixed<1>, dev::k_c2r_mixed<2>);
+    auto* fn = kernelsFor(half, m).c2r;
     if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
     const uint64_t groups = (batch + m.rows - 1) / m.rows;
@@ -454,7 +619,7 @@ int launchStftMixed(const void* sig, void* out, const MixedRadix& half, uint64_t
                     const void* tw, const void* twr, void* stream) {
     if (!mixedValid(half)) return (int)cudaErrorInvalidValue;
     const MixedShape m = mixedShape(half);
-    auto* fn = byClass(m.cls, dev::k_stft_mixed<0>, dev::k_stft_mixed<1>, dev::k_stft_mixed<2>);
+    auto* fn = kernelsFor(half, m).stft;
     if (m.smem > kMixedMaxSmem) return (int)cudaErrorInvalidValue;
     if (int e = optInSharedMemory((const void*)fn, kMixedMaxSmem)) return e;
     const uint64_t frames = signals * framesPerSignal;
@@ -484,8 +649,8 @@ int launchIstftMixed(const void* spec, void* out, const MixedRadix& half, uint64
     // and window (a frame of N % 4 == 2 would read past its row)
     const bool vec = N % 4 == 0 && hop % 4 == 0 && outLen % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15u) == 0 &&
                      (reinterpret_cast<uintptr_t>(window) & 15u) == 0;
-    auto* fn = vec ? byClass(m.cls, dev::k_istft_mixed<0, 4>, dev::k_istft_mixed<1, 4>, dev::k_istft_mixed<2, 4>)
-                   : byClass(m.cls, dev::k_istft_mixed<0, 1>, dev::k_istft_mixed<1, 1>, dev::k_istft_mixed<2, 1>);
+    const MixedKernels k = kernelsFor(half, m);
+    auto* fn = vec ? k.istft4 : k.istft1;
     if (int e = optInSharedMemory((const void*)fn, kMaxSmem)) return e;
     int device = 0, sms = 0, perSm = 0;
     if (cudaGetDevice(&device) != cudaSuccess ||
