@@ -74,6 +74,9 @@ int launchLongA(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
                 bool inverse, const void* tw1, const void* tlo, const void* thi, void* stream);
 int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t batch,
                 bool inverse, float scale, const void* tw2, void* stream);
+// Load every pass-A and pass-B variant on the current device and opt each into its shared
+// memory, so that later launches neither load device code nor set kernel attributes.
+int prepareLongKernels();
 
 // Single-pass long C2C: one thread-block cluster per row, transpose through distributed
 // shared memory (n in 8192..65536; tw1 = Stockham (n/256, 16), tw2 = Stockham (256, 16)).

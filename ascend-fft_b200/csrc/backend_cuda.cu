@@ -216,13 +216,29 @@ int launchLongA(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
                 bool inverse, const void* tw1, const void* tlo, const void* thi, void* stream) {
     const Entry* x = dev::findLongA(n1, inverse);
     if (!x || n2 % (uint32_t)x->rows) return (int)cudaErrorInvalidDeviceFunction;
+    const uint64_t perRow = n2 / (uint32_t)x->rows;
+    if (batch == 0 || batch > 0x7fffffffull / perRow) return (int)cudaErrorInvalidValue;
     if (int err = prepareEntry(x)) return err;
     auto fn = reinterpret_cast<dev::KLongA>(const_cast<void*>(x->fn));
-    const uint64_t grid = batch * (n2 / (uint32_t)x->rows);
+    const uint64_t grid = batch * perRow;
     fn<<<(unsigned)grid, x->cta, x->smem, S(stream)>>>(
         static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw1),
         static_cast<const float2*>(tlo), static_cast<const float2*>(thi), batch, ilog2u(n2));
     return rc(cudaGetLastError());
+}
+
+int prepareLongKernels() {
+    for (uint32_t n1 = 32; n1 <= 256; n1 *= 2)
+        for (int inv = 0; inv < 2; ++inv) {
+            const Entry* xs[2] = {dev::findLongA(n1, inv != 0), n1 == 256 ? dev::findLongB(256, inv != 0) : nullptr};
+            for (const Entry* x : xs) {
+                if (!x) continue;
+                cudaFuncAttributes attr;
+                if (int err = rc(cudaFuncGetAttributes(&attr, x->fn))) return err;   // loads the kernel
+                if (int err = prepareEntry(x)) return err;
+            }
+        }
+    return 0;
 }
 
 bool hasCols(uint32_t ny) { return dev::findCols(ny, false) != nullptr; }
@@ -246,9 +262,11 @@ int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
                 bool inverse, float scale, const void* tw2, void* stream) {
     const Entry* x = dev::findLongB(n2, inverse);
     if (!x || n1 % (uint32_t)x->rows) return (int)cudaErrorInvalidDeviceFunction;
+    const uint64_t perRow = n1 / (uint32_t)x->rows;
+    if (batch == 0 || batch > 0x7fffffffull / perRow) return (int)cudaErrorInvalidValue;
     if (int err = prepareEntry(x)) return err;
     auto fn = reinterpret_cast<dev::KLongB>(const_cast<void*>(x->fn));
-    const uint64_t grid = batch * (n1 / (uint32_t)x->rows);
+    const uint64_t grid = batch * perRow;
     fn<<<(unsigned)grid, x->cta, x->smem, S(stream)>>>(
         static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw2),
         batch, ilog2u(n1), scale);

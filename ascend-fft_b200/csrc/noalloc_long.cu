@@ -14,9 +14,10 @@
 //    are rejected with status -12 before any GPU work;
 //  * every GPU that loads this library keeps the 32 MiB array (plus 18 KB of tables)
 //    until the process exits;
-//  * the first call on a device looks up the arrays' device addresses, builds the twiddle
-//    tables on the caller's stream and waits for that stream once; make that first call
-//    before any stream capture;
+//  * the first call on a device looks up the arrays' device addresses, loads every kernel
+//    variant it can launch, builds the twiddle tables on the caller's stream and waits for
+//    that stream once; make that first call before any stream capture (a first call on a
+//    stream that is being captured returns -13 and leaves the capture untouched);
 //  * all calls share one workspace: calls whose executions overlap on the GPU (different
 //    streams, or different host threads) race and corrupt each other's results.  Nothing in
 //    the workspace needs to start at zero: the column pass writes every value the row pass
@@ -57,12 +58,23 @@ static std::mutex g_mutex;
 static DeviceState g_state[64];
 
 // Set-up on the current device: symbol addresses (host code must not use the array names as
-// addresses) and the FP64-built twiddle tables, built on `stream` and waited for once.
-static int setup(int device, cudaStream_t stream, DeviceState* st) {
+// addresses), every four-step kernel variant this entry point can launch loaded and opted into
+// its shared memory (so no later call loads device code or changes a kernel attribute), and the
+// FP64-built twiddle tables, built on `stream` and waited for once.  A stream that is being
+// captured is refused before anything touches it (-13): the table builds and the wait would
+// land in, and break, the caller's capture.
+static int setup(cudaStream_t stream, DeviceState* st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return -13;
+    }
+    if (cs != cudaStreamCaptureStatusNone) return -13;
     void* scratch = nullptr;
     void* tables = nullptr;
     if (cudaGetSymbolAddress(&scratch, g_scratch) != cudaSuccess) return -1;
     if (cudaGetSymbolAddress(&tables, g_tables) != cudaSuccess) return -1;
+    if (bfly::backend::prepareLongKernels()) return -1;
     float2* t = static_cast<float2*>(tables);
     dev::k_tw_stockham<32, 16><<<1, 256, 0, stream>>>(t + kTw1[0]);
     dev::k_tw_stockham<64, 16><<<1, 256, 0, stream>>>(t + kTw1[1]);
@@ -76,7 +88,6 @@ static int setup(int device, cudaStream_t stream, DeviceState* st) {
     }
     if (cudaGetLastError() != cudaSuccess) return -1;
     if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
-    (void)device;
     st->scratch = static_cast<float2*>(scratch);
     st->tables = t;
     st->ready = true;
@@ -92,7 +103,7 @@ extern "C" int bfly_exec_c2c_long_noalloc(const void* d_in, void* d_out, uint32_
     if (!d_in || !d_out) return -10;
     if (n < 8192 || n > 65536 || (n & (n - 1)) || batch == 0 || (direction != -1 && direction != 1))
         return -8;
-    if ((unsigned long long)n * batch > kScratchElems) return -12;
+    if (batch > kScratchElems / n) return -12;   // n >= 8192 here; the product could wrap
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return -1;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -100,7 +111,7 @@ extern "C" int bfly_exec_c2c_long_noalloc(const void* d_in, void* d_out, uint32_
     {
         std::lock_guard<std::mutex> lock(g_mutex);
         if (!g_state[device].ready) {
-            if (int r = setup(device, s, &g_state[device])) return r;
+            if (int r = setup(s, &g_state[device])) return r;
         }
         st = g_state[device];
     }

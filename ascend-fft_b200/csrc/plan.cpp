@@ -740,7 +740,7 @@ int Plan::execC2C2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint6
                     int direction, float scale, void* stream) {
     if (!dIn || !dOut || batch == 0 || (direction != -1 && direction != 1)) return -8;
     if (!pow2(ny) || !backend::hasCols(ny)) return -8;
-    if (batch * ny > 0xFFFFFFFFull || !validShape(nx, (uint32_t)(batch * ny), kExecC2C)) return -8;
+    if (batch > 0xFFFFFFFFull / ny || !validShape(nx, (uint32_t)(batch * ny), kExecC2C)) return -8;
     if (int r = execC2CWith(dIn, dOut, nx, batch * ny, direction, 1.0f, stream, nullptr)) return r;
     return execCols(dOut, dOut, ny, batch, nx, nx, direction > 0, scale, stream);
 }
@@ -844,7 +844,7 @@ int Plan::execC2R(const void* dIn, void* dOut, uint32_t n, uint64_t batch, float
 int Plan::execR2C2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch, float scale,
                     void* stream) {
     if (!dIn || !dOut || batch == 0 || !pow2(ny) || !backend::hasCols(ny)) return -8;
-    if (batch * ny > 0xFFFFFFFFull) return -8;
+    if (batch > 0xFFFFFFFFull / ny) return -8;
     const uint32_t half = nx / 2 + 1;
     if (int r = execR2C(dIn, dOut, nx, batch * ny, 1.0f, 1.0f, stream)) return r;
     return execCols(dOut, dOut, ny, batch, half, half, false, scale, stream);
@@ -853,7 +853,7 @@ int Plan::execR2C2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint6
 int Plan::execC2R2D(const void* dIn, void* dOut, uint32_t ny, uint32_t nx, uint64_t batch, float scale,
                     void* stream) {
     if (!dIn || !dOut || batch == 0 || !pow2(ny) || !backend::hasCols(ny)) return -8;
-    if (batch * ny > 0xFFFFFFFFull || !validShape(nx, (uint32_t)(batch * ny), kExecC2R)) return -8;
+    if (batch > 0xFFFFFFFFull / ny || !validShape(nx, (uint32_t)(batch * ny), kExecC2R)) return -8;
     const uint32_t half = nx / 2 + 1;
     if (ensureBuf(&impl_->devHalf, &impl_->devHalfCap, (size_t)batch * ny * half * 8)) return -3;
     if (int r = execCols(dIn, impl_->devHalf, ny, batch, half, half, true, 1.0f, stream)) return r;

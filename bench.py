@@ -1,26 +1,33 @@
-"""Benchmark of the batched FFT library on B200 (one JSON line on rank 0).
+"""Benchmark of the batched FFT library on B200.
 
-Workload (the configuration the headline metric is quoted on): plain fp32 C2C forward over
-the 49-point grid N in {64..4096} x batch in {1..4096}, interleaved complex, Re/Im i.i.d.
-N(0,1) seeded per point (seed = 1000*log2 N + log2 batch + 1).  One step = one forward
-transform of every grid point on inputs resident in HBM, run as ONE ragged launch
-(k_ragged_flat over the 49 requests: 10,931 tiles of 4096 or 2048 points, one per CTA).  The step touches 355 MB of input and 355 MB of output, more
-than the 126 MB L2, so no explicit flush is needed between steps.  The same step as 49
-per-point launches replayed from a CUDA graph is reported beside it (per_point_graph).
+Output: JSON lines on rank 0.  Every line but the last is a sub-measurement tagged "sub"; the
+LAST line is the headline (kept under 2 KB), and the line before it ("sub": "summary") holds the
+key figures of every sub-measurement, so both survive a reader that keeps only the end of the
+output.
+
+Headline workload (the configuration the metric is quoted on): plain fp32 C2C forward over the
+49-point grid N in {64..4096} x batch in {1..4096}, interleaved complex, Re/Im i.i.d. N(0,1)
+seeded per point (seed = 1000*log2 N + log2 batch + 1).  One step = one forward transform of
+every grid point on inputs resident in HBM, run as ONE ragged launch (k_ragged_flat over the 49
+requests: 10,931 tiles of 4096 or 2048 points, one per CTA).  The step touches 355 MB of input
+and 355 MB of output, more than the 126 MB L2, so no explicit flush is needed between steps.
 
   value      algorithmic bytes (16 * N * batch summed over the grid) / device time per step
-  e2e        the same metric through the C ABI's synchronous host-pointer entry points with
-             pinned host buffers, H2D + kernels + D2H inside the timed step: the whole grid in
-             one bfly_plan_run_c2c_many call (value), and one bfly_plan_run_c2c call per point
-             as the reference calls it (per_call)
-  roofline   the step's only kernel (k_ragged_flat over the grid) timed with CUDA events on its
-             stream against the measured HBM copy bandwidth; the largest single-size launch
-             (N=4096, batch=4096, k_c2c) is reported beside it (largest_launch)
+  e2e        the same metric through the C ABI's synchronous host-pointer entry point with
+             pinned host buffers, H2D + kernels + D2H inside the timed step (the whole grid in
+             one bfly_plan_run_c2c_many call); `scopes` splits it into event spans
+  roofline   the step's only kernel timed with CUDA events on its stream against the measured
+             HBM copy bandwidth
   cpu_baseline  the reference's own CPU FFT (its FP64 oracle src/framework/reference.cpp,
-             compiled from its sources into oracle/_ref) on a bounded sample of the grid,
-             rows spread over the host's threads
+             compiled from its sources into oracle/_ref) on a bounded sample of the grid
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Sub-measurements (one line each): c2c_grid49_points (every grid point as its own launch, fp32
+and split-BF16 tensor cores), ragged_mix256 (the 256-request seed-7 mix, one launch vs one launch
+per request, CUDA graphs), real_r2c_c2r (R2C N 128..8192 and C2R N 64..4096 at batch 1, 64, 1024),
+long_fwd_bwd, c2c_2d, c2c_any_length, stft, cpu_stdlib (numpy / torch CPU FFT with the
+reference's protocol: 3 warm-ups, 20 reps, mean and min).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-extras]
 Under torchrun every rank runs the grid on its own GPU (weak scaling; no data-path
 collective) and rank 0 prints the max-over-ranks time.
 """
@@ -53,12 +60,45 @@ WORKLOAD = ("c2c_fwd_grid49: plain fp32 C2C forward over N{64..4096} x batch{1..
             "interleaved complex64, N(0,1) seeded per point")
 
 
+def emit(obj):
+    print(json.dumps(obj, separators=(",", ":")), flush=True)
+
+
 def grid_seed(n, b):
     return 1000 * (n.bit_length() - 1) + (b.bit_length() - 1) + 1
 
 
 def grid_bytes():
     return sum(16 * n * b for n in GRID_N for b in GRID_B)
+
+
+def mix256(count: int = 256, seed: int = 7):
+    """The ragged request mix: log2 n ~ U{6..12}, batch = round(2^U(0,9)), then the OFDM-like
+    2048 x (14*100), radar-like 512 x 4096 and spectral-layer-like 1024 x (8*768) groups of the
+    reference's application proxies (scripts/e2e_test.py:94-102)."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for _ in range(count - 3):
+        n = 1 << int(rng.integers(6, 13))
+        b = max(1, int(round(2.0 ** rng.uniform(0.0, 9.0))))
+        reqs.append((n, b))
+    return reqs + [(2048, 14 * 100), (512, 4096), (1024, 8 * 768)]
+
+
+def sample_rows(batch: int, want: int):
+    """Evenly spread row indices including the first and the last."""
+    if batch <= want:
+        return list(range(batch))
+    if want == 1:
+        return [0]
+    return [i * (batch - 1) // (want - 1) for i in range(want)]
+
+
+def rel_l2_rows(got, ref):
+    """Maximum over rows of the relative L2 error against an FP64 result."""
+    d = np.linalg.norm(np.asarray(got).astype(np.complex128) - ref, axis=-1)
+    r = np.linalg.norm(ref, axis=-1)
+    return float((d / np.where(r > 0, r, 1.0)).max()) if d.size else 0.0
 
 
 def load_peaks():
@@ -69,21 +109,21 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def dominant_traffic():
-    """DRAM bytes of one full-grid launch of the step's kernel: the committed ncu capture of the
-    capped grid (profiles/roofline_traffic.txt) scaled by algorithmic bytes, or None."""
+def grid_traffic():
+    """DRAM bytes read and written inside one launch of the step's kernel over the full grid,
+    from the committed ncu capture (profiles/roofline_traffic.txt), or (None, None)."""
     p = ROOT / "profiles" / "roofline_traffic.txt"
     if not p.exists():
-        return None
+        return None, None
     vals = {}
     for line in p.read_text().splitlines():
         parts = line.split()
         if len(parts) == 2 and not parts[0].startswith("#"):
             vals[parts[0]] = int(parts[1])
-    t, a = vals.get("ragged_grid49_cap1024"), vals.get("ragged_grid49_cap1024_algorithmic")
-    if not t or not a:
-        return None
-    return int(round(t * grid_bytes() / a))
+    r, w = vals.get("ragged_grid49_dram_read"), vals.get("ragged_grid49_dram_write")
+    if r is None or w is None:
+        return None, None
+    return r, w
 
 
 # ------------------------------------------------------------------ clocks
@@ -170,7 +210,8 @@ class ClockSampler:
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
         return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+                "reasons": sorted(self.reasons), "samples": len(self.samples),
+                "samples_in_timed_region": getattr(self, "in_region", len(self.samples))}
 
 
 # ------------------------------------------------------------------ CPU reference
@@ -223,26 +264,36 @@ def cpu_reference_sample(rows_cap: int, budget_s: float, threads: int):
     return nbytes * reps / dt / 1e9, dt, nbytes * reps, kind, desc
 
 
-def stdlib_numpy_sample(budget_s: float):
-    """numpy.fft.fft on complex64 (the reference's stdlib baseline, scripts/bench_stdlib.py),
-    single-threaded pocketfft, on the grid capped at 64 rows per point."""
-    xs = []
-    for n in GRID_N:
-        for b in GRID_B:
-            rng = np.random.default_rng(grid_seed(n, b))
-            z = rng.standard_normal((min(b, 64), 2 * n)).astype(np.float32).view(np.complex64)
-            xs.append(z)
-    nbytes = sum(16 * z.size for z in xs)
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        for z in xs:
-            np.fft.fft(z, axis=-1)
-        reps += 1
-        if time.perf_counter() - t0 >= budget_s:
-            break
-    dt = time.perf_counter() - t0
-    return nbytes * reps / dt / 1e9
+def cpu_stdlib(reps: int = 20):
+    """The reference's stdlib baseline protocol (scripts/bench_stdlib.py:18-46): numpy.fft.fft
+    on complex64 along the last axis and torch.fft.fft on CPU, 3 warm-up calls, then `reps`
+    timed calls, mean and min in microseconds; on the config-1 shape (N=1024, B=256, U[-1,1)
+    seed 0) and the reference's default grid N {256, 1024, 4096} x B {1, 64, 4096}."""
+    import torch
+
+    def bench(fn, x):
+        for _ in range(3):
+            fn(x)
+        ts = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            fn(x)
+            ts.append(time.perf_counter() - t)
+        return round(sum(ts) / len(ts) * 1e6, 1), round(min(ts) * 1e6, 1)
+
+    shapes = [(1024, 256)] + [(n, b) for n in (256, 1024, 4096) for b in (1, 64, 4096)]
+    rows = []
+    for n, b in shapes:
+        rng = np.random.default_rng(0 if (n, b) == (1024, 256) else grid_seed(n, b))
+        x = rng.uniform(-1.0, 1.0, size=(b, 2 * n)).astype(np.float32).view(np.complex64)
+        nu, nmin = bench(lambda z: np.fft.fft(z, axis=-1), x)
+        t = torch.from_numpy(x.copy())
+        tu, tmin = bench(lambda z: torch.fft.fft(z), t)
+        rows.append([n, b, nu, nmin, tu, tmin])
+    return {"sub": "cpu_stdlib", "protocol": "3 warm-ups, 20 reps, mean/min us (scripts/bench_stdlib.py)",
+            "cols": ["n", "b", "numpy_us", "numpy_min_us", "torch_us", "torch_min_us"], "rows": rows,
+            "numpy": np.__version__, "torch": torch.__version__, "torch_threads": torch.get_num_threads(),
+            "cpu_count": os.cpu_count()}
 
 
 # ------------------------------------------------------------------ distributed helpers
@@ -274,195 +325,295 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "sample": "rows per grid point capped at 256",
                        "points": len(GRID_N) * len(GRID_B)},
+            "same_config": False,
+            "same_config_note": ("the reference's CPU FFT runs every grid point with its rows capped at "
+                                 "256 (110.9 MB per step against the GPU arm's 710.2 MB); GB/s is per "
+                                 "algorithmic byte on both arms"),
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": desc},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
 
 
-# ------------------------------------------------------------------ our arm
-def extra_measurements(dev, stream):
-    """Forms beside the plain fp32 grid (single GPU): split-BF16 tensor cores (3 and 2 bf16
-    terms) vs fp32 at every point of the 49-point grid; long C2C forward + backward (batch*n =
-    2^26; single pass up to n = 16384, four-step above); 2-D C2C at the reference's planned 2-D /
-    range-Doppler shapes and transforms along a middle axis; non-power-of-two C2C (prime-factor,
-    mixed-radix, Bluestein); STFT and inverse STFT; real transforms forward + adjoint at batch
-    1024.  Each figure: algorithmic GB/s from CUDA
-    events on `stream` around one replay of a CUDA graph holding 20 launches (after 3 warm-up
-    launches), and the error against FP64 on sampled rows."""
-    import torch
-    import bfly
-    import oracle.fft_oracle as O
-    sh = stream.cuda_stream
-    peak, _ = load_peaks()
+# ------------------------------------------------------------------ sub-measurements
+class Subs:
+    """Sub-measurements beside the headline (one GPU).  Each figure is device time from CUDA
+    events on `stream` around one replay of a CUDA graph holding `reps` launches (after 3 warm-up
+    launches outside the capture), and the error against an FP64 numpy FFT on sampled rows."""
 
-    def timed(fn, reps=20):
-        # warm-up outside the capture (table builds, workspaces), then `reps` launches captured
-        # in one CUDA graph and replayed: the figure is device time, not Python call rate
+    def __init__(self, dev, stream, ctx, plan):
+        import torch
+        self.torch = torch
+        self.dev, self.stream, self.sh = dev, stream, stream.cuda_stream
+        self.ctx, self.plan = ctx, plan
+        self.peak, _ = load_peaks()
+        self.summary = {}
+
+    def timed(self, fn, reps=20):
+        torch = self.torch
         for _ in range(3):
             fn()
-        stream.synchronize()
+        self.stream.synchronize()
         graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph, stream=stream):
+        with torch.cuda.graph(graph, stream=self.stream):
             for _ in range(reps):
                 fn()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
+        with torch.cuda.stream(self.stream):
             graph.replay()
-            e0.record(stream)
+            e0.record(self.stream)
             graph.replay()
-            e1.record(stream)
+            e1.record(self.stream)
         e1.synchronize()
         del graph
         return e0.elapsed_time(e1) / reps
 
-    def rel(y, x, inverse=False, rows=4):
-        idx = O.sample_batches(x.shape[0], rows)
+    def gbs(self, nbytes, ms):
+        return nbytes / (ms / 1e3) / 1e9
+
+    def err(self, y, x, inverse=False, rows=4, scale=1.0):
+        idx = sample_rows(x.shape[0], rows)
         xs = x[idx].cpu().numpy().astype(np.complex128)
-        ref = np.fft.ifft(xs, axis=-1) * xs.shape[-1] if inverse else np.fft.fft(xs, axis=-1)
-        return O.rel_l2_rows(y[idx].cpu().numpy(), ref)
+        ref = np.fft.ifft(xs, axis=-1) * xs.shape[-1] * scale if inverse else np.fft.fft(xs, axis=-1)
+        return rel_l2_rows(y[idx].cpu().numpy(), ref)
 
-    out = {"split_bf16": {}, "long_fwd_bwd": {}, "real_fwd_adjoint": {}}
-    # ---- split-BF16 tensor cores vs plain fp32 at every point of the 49-point grid
-    for n, b in ((n, b) for n in GRID_N for b in GRID_B):
-        g = torch.Generator(device=dev).manual_seed(grid_seed(n, b))
-        x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
-        y = torch.empty_like(x)
-        byts = 16 * n * b
-        plan = bfly.plan_for(dev, n)
+    def check(self, r, what):
+        if r:
+            raise RuntimeError(f"{what}: status {r}")
+
+    # -- config 2: every grid point as its own launch, fp32 and split-BF16
+    def grid_points(self):
+        torch, sh, peak = self.torch, self.sh, self.peak
+        import bfly
+        rows, best = [], None
+        for n in GRID_N:
+            for b in GRID_B:
+                g = torch.Generator(device=self.dev).manual_seed(grid_seed(n, b))
+                x = torch.randn(b, n, dtype=torch.complex64, device=self.dev, generator=g)
+                y = torch.empty_like(x)
+                plan = bfly.plan_for(self.dev, n)
+                byts = 16 * n * b
+                res = []
+                for split in (0, 3, 2):
+                    if split:
+                        fn = lambda: self.check(plan.exec_c2c_tc(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, split, sh), "tc")
+                    else:
+                        fn = lambda: self.check(plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh), "c2c")
+                    ms = self.timed(fn)
+                    res.append((ms, self.gbs(byts, ms), self.err(y, x)))
+                (ms0, g0, e0), (_, g3, e3), (_, g2, e2) = res
+                rows.append([n, b, round(ms0 * 1e3, 2), round(g0, 1), round(g0 / peak, 3), float(f"{e0:.3g}"),
+                             round(g3, 1), float(f"{e3:.3g}"), round(g2, 1), float(f"{e2:.3g}")])
+                sp = g3 / g0
+                if best is None or sp > best[0]:
+                    best = (sp, n, b, e3)
+                del x, y
+        meets = sum(1 for r in rows if r[4] >= 0.70)
+        emit({"sub": "c2c_grid49_points", "unit": UNIT, "peak": peak,
+              "cols": ["n", "b", "fp32_us", "fp32_gbs", "fp32_frac", "fp32_rel_l2", "tc3_gbs", "tc3_rel_l2",
+                       "tc2_gbs", "tc2_rel_l2"], "rows": rows, "fp32_points_at_0.70": meets,
+              "l2": "points under 126 MB are L2-warm across the 20 back-to-back launches of the graph"})
+        b4096 = [r for r in rows if r[1] == 4096]
+        self.summary["grid49_points"] = {
+            "fp32_frac_at_b4096": [r[4] for r in b4096], "fp32_points_at_0.70": meets,
+            "tc3_vs_fp32_at_b4096": [round(r[6] / r[3], 2) for r in b4096],
+            "tc3_best_speedup": [round(best[0], 3), best[1], best[2]],
+            "tc3_max_rel_l2": max(r[7] for r in rows), "tc2_max_rel_l2": max(r[9] for r in rows)}
+
+    # -- config 4: the 256-request mix in one launch, against one launch per request
+    def ragged_mix(self):
+        torch, sh, peak = self.torch, self.sh, self.peak
+        reqs = mix256()
+        g = torch.Generator(device=self.dev).manual_seed(7)
+        bufs = []
+        for n, b in reqs:
+            x = torch.randn(b, n, dtype=torch.complex64, device=self.dev, generator=g)
+            bufs.append((n, b, x, torch.empty_like(x)))
+        plan = self.plan
+        for n, b, _, _ in bufs:
+            self.check(plan.prepare(n, b), "prepare")
+        total = sum(16 * n * b for n, b, _, _ in bufs)
+        ragged = plan.make_ragged((x.data_ptr(), y.data_ptr(), n, b, -1, 1.0) for n, b, x, y in bufs)
+        ms_r = self.timed(lambda: self.check(ragged.exec(sh), "ragged"), reps=10)
+        worst = 0.0
+        for n, b, x, y in bufs[::16] + bufs[-3:]:
+            worst = max(worst, self.err(y, x, rows=2))
+
+        import bfly
+        plans = {n: bfly.plan_for(self.dev, n) for n, _ in reqs}   # each length's measured best plan
+
+        def per_request():
+            for n, b, x, y in bufs:
+                self.check(plans[n].exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh), "c2c")
+        ms_p = self.timed(per_request, reps=2)
+        # the same launches issued one by one from the host (no graph)
+        for _ in range(2):
+            with torch.cuda.stream(self.stream):
+                per_request()
+        self.stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        for _ in range(3):
+            per_request()
+        e1.record(self.stream)
+        e1.synchronize()
+        ms_e = e0.elapsed_time(e1) / 3
+        info = ragged.info()
+        ragged.close()
+        r = {"requests": len(reqs), "bytes": total, "tiles": info["tiles"],
+             "one_launch_gbs": round(self.gbs(total, ms_r), 1), "one_launch_frac": round(self.gbs(total, ms_r) / peak, 3),
+             "one_launch_us": round(ms_r * 1e3, 1), "per_request_graph_gbs": round(self.gbs(total, ms_p), 1),
+             "per_request_eager_gbs": round(self.gbs(total, ms_e), 1),
+             "speedup_vs_per_request_graph": round(ms_p / ms_r, 2),
+             "speedup_vs_per_request_eager": round(ms_e / ms_r, 2), "rel_l2_max": float(f"{worst:.3g}")}
+        emit({"sub": "ragged_mix256", "unit": UNIT, "seed": 7,
+              "mode": "one k_ragged_flat launch replayed from a CUDA graph", **r})
+        self.summary["ragged_mix256"] = {k: r[k] for k in ("one_launch_gbs", "one_launch_frac",
+                                                           "speedup_vs_per_request_graph",
+                                                           "speedup_vs_per_request_eager", "rel_l2_max")}
+        del bufs
+
+    # -- config 3: R2C N 128..8192 and C2R N 64..4096 at batch 1, 64, 1024
+    def real_transforms(self):
+        torch, sh, peak = self.torch, self.sh, self.peak
+        import bfly
+        r2c, c2r = [], []
+        for kind, ns in (("r2c", [128 << i for i in range(7)]), ("c2r", [64 << i for i in range(7)])):
+            for n in ns:
+                plan = bfly.plan_for(self.dev, n, "real")
+                for b in (1, 64, 1024):
+                    rng = np.random.default_rng(n * 7 + b)
+                    xr = rng.uniform(-1.0, 1.0, size=(b, n))
+                    byts = (8 * n + 8) * b
+                    if kind == "r2c":
+                        x = torch.from_numpy(xr.astype(np.float32)).to(self.dev)
+                        y = torch.empty(b, n // 2 + 1, dtype=torch.complex64, device=self.dev)
+                        ms = self.timed(lambda: self.check(plan.exec_r2c(x.data_ptr(), y.data_ptr(), n, b, 1.0, 1.0, sh), "r2c"))
+                        idx = sample_rows(b, 4)
+                        ref = np.fft.rfft(x[idx].cpu().numpy().astype(np.float64), axis=-1)
+                        e = rel_l2_rows(y[idx].cpu().numpy(), ref)
+                        r2c.append([n, b, round(ms * 1e3, 2), round(self.gbs(byts, ms), 1), float(f"{e:.3g}")])
+                    else:
+                        X = np.fft.rfft(xr, axis=-1)
+                        X[:, 0] = X[:, 0].real
+                        X[:, -1] = X[:, -1].real
+                        x = torch.from_numpy(X.astype(np.complex64)).to(self.dev)
+                        y = torch.empty(b, n, device=self.dev)
+                        ms = self.timed(lambda: self.check(plan.exec_c2r(x.data_ptr(), y.data_ptr(), n, b, 1.0, 1.0, 1.0 / n, sh), "c2r"))
+                        idx = sample_rows(b, 4)
+                        ref = np.fft.irfft(X[idx].astype(np.complex64).astype(np.complex128), n=n, axis=-1)
+                        e = rel_l2_rows(y[idx].cpu().numpy(), ref)
+                        c2r.append([n, b, round(ms * 1e3, 2), round(self.gbs(byts, ms), 1), float(f"{e:.3g}")])
+                    del x, y
+        emit({"sub": "real_r2c_c2r", "unit": UNIT, "bytes": "(8n+8)*batch", "cols": ["n", "b", "us", "gbs", "rel_l2"],
+              "r2c": r2c, "c2r": c2r,
+              "inputs": "R2C U[-1,1); C2R the rfft of seeded U[-1,1) reals with DC/Nyquist imag zeroed"})
+        self.summary["real_r2c_c2r_b1024"] = {
+            "r2c_gbs": [r[3] for r in r2c if r[1] == 1024], "c2r_gbs": [r[3] for r in c2r if r[1] == 1024],
+            "max_rel_l2": max(r[4] for r in r2c + c2r)}
+
+    # -- config 5: long C2C forward + backward (the conjugate-FFT adjoint), batch * n = 2^26
+    def long_fwd_bwd(self):
+        torch, sh, peak = self.torch, self.sh, self.peak
+        import bfly
         res = {}
-        for tag, fn in (("fp32", lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh)),
-                        ("tc_split3", lambda: plan.exec_c2c_tc(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, 3, sh)),
-                        ("tc_split2", lambda: plan.exec_c2c_tc(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, 2, sh))):
-            ms = timed(fn)
-            gbs = byts / (ms / 1e3) / 1e9
-            res[tag] = {"gbs": round(gbs, 1), "frac": round(gbs / peak, 4), "rel_l2": rel(y, x)}
-        res["speedup_split3_vs_fp32"] = round(res["tc_split3"]["gbs"] / res["fp32"]["gbs"], 3)
-        res["speedup_split2_vs_fp32"] = round(res["tc_split2"]["gbs"] / res["fp32"]["gbs"], 3)
-        out["split_bf16"][f"n{n}_b{b}"] = res
-        del x, y
-    # ---- long C2C forward + backward (the backward is the conjugate-FFT adjoint)
-    for n in (8192, 16384, 32768, 65536):
-        b = (1 << 26) // n
-        g = torch.Generator(device=dev).manual_seed(11)
-        x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
-        y = torch.empty_like(x)
-        z = torch.empty_like(x)
-        plan = bfly.plan_for(dev, n)
-        byts = 16 * n * b
-        ms_f = timed(lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh))
-        ms_b = timed(lambda: plan.exec_c2c(y.data_ptr(), z.data_ptr(), n, b, 1, 1.0, sh))
-        out["long_fwd_bwd"][f"n{n}_b{b}"] = {
-            "fwd_gbs": round(byts / (ms_f / 1e3) / 1e9, 1), "bwd_gbs": round(byts / (ms_b / 1e3) / 1e9, 1),
-            "fwd_bwd_gbs": round(2 * byts / ((ms_f + ms_b) / 1e3) / 1e9, 1),
-            "fwd_rel_l2": rel(y, x, rows=2), "bwd_rel_l2": rel(z, y, inverse=True, rows=2),
-            "schedule": "single pass" if n <= 16384 else "four-step (2 HBM passes)"}
-        del x, y, z
-    # ---- 2-D C2C (row pass + column pass) at the reference's planned 2-D / range-Doppler
-    # shapes, batch * ny * nx = 2^26; and transforms along the middle axis of [outer][n][inner]
-    out["c2c_2d"] = {}
-    for ny, nx in ((256, 256), (512, 512), (1024, 1024), (2048, 2048), (1024, 128), (128, 1024)):
-        b = (1 << 26) // (ny * nx)
-        g = torch.Generator(device=dev).manual_seed(ny + nx)
-        x = torch.randn(b, ny, nx, dtype=torch.complex64, device=dev, generator=g)
-        y = torch.empty_like(x)
-        plan = bfly.plan_for(dev, nx)
-        ms = timed(lambda: plan.exec_c2c_2d(x.data_ptr(), y.data_ptr(), ny, nx, b, -1, 1.0, sh))
-        xs = x[:1].cpu().numpy().astype(np.complex128)
-        ref = np.fft.fft2(xs).reshape(1, -1)
-        err = float(np.linalg.norm(y[:1].cpu().numpy().reshape(1, -1) - ref) / np.linalg.norm(ref))
-        out["c2c_2d"][f"{ny}x{nx}_b{b}"] = {"gbs": round(16 * ny * nx * b / ms / 1e6, 1),
-                                           "frac": round(16 * ny * nx * b / ms / 1e6 / peak, 4),
-                                           "rel_l2": err, "passes": 2}
-        del x, y
-    for n, outer, inner in ((1024, 64, 1024), (256, 1024, 256)):
-        g = torch.Generator(device=dev).manual_seed(n + inner)
-        x = torch.randn(outer, n, inner, dtype=torch.complex64, device=dev, generator=g)
-        y = torch.empty_like(x)
-        plan = bfly.plan_for(dev, n)
-        ms = timed(lambda: plan.exec_c2c_axis(x.data_ptr(), y.data_ptr(), n, outer, inner, -1, 1.0, sh))
-        xs = x[:1].cpu().numpy().astype(np.complex128)
-        ref = np.fft.fft(xs, axis=1)
-        err = float(np.linalg.norm(y[:1].cpu().numpy() - ref) / np.linalg.norm(ref))
-        out["c2c_2d"][f"axis_n{n}_outer{outer}_inner{inner}"] = {
-            "gbs": round(16 * n * outer * inner / ms / 1e6, 1),
-            "frac": round(16 * n * outer * inner / ms / 1e6 / peak, 4), "rel_l2": err, "passes": 1}
-        del x, y
-    # ---- non-power-of-two C2C, batch * n ~ 2^25: prime-factor kernel (n = A * 2^k) and
-    # Bluestein (other lengths), one kernel each
-    out["c2c_any_length"] = {}
-    for n in (1536, 1920, 6144, 360, 1000, 3000, 6561, 12000, 1001, 1003, 8191):
-        b = (1 << 25) // n
-        g = torch.Generator(device=dev).manual_seed(n)
-        x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
-        y = torch.empty_like(x)
-        plan = bfly.plan_for(dev, n)
-        ms = timed(lambda: plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh))
-        gbs = 16 * n * b / ms / 1e6
-        pfa = any(n % a == 0 and (n // a) & (n // a - 1) == 0 and n // a >= 16 for a in (3, 5, 9, 15))
-        m = n
-        for p in (2, 3, 5, 7, 11, 13):
-            while m % p == 0:
-                m //= p
-        kernel = ("prime-factor" if pfa else "mixed-radix" if m == 1 and n <= 12288
-                  else f"bluestein (padded length {1 << (2 * n - 2).bit_length()})")
-        out["c2c_any_length"][f"n{n}_b{b}"] = {
-            "gbs": round(gbs, 1), "frac": round(gbs / peak, 4), "rel_l2": rel(y, x), "kernel": kernel}
-        del x, y
-    # ---- STFT (frame gather + Hann window + one-sided transform in one kernel), 4 signals of
-    # 2^24 samples, centred; bytes counted per frame as the reference's dense-frame R2C proxy
-    out["stft"] = {}
-    plan = bfly.plan_for(dev, 1024, "real")
-    for n, hop in ((256, 64), (1024, 256), (4096, 1024), (400, 160)):
-        L, S = 1 << 24, 4
-        g = torch.Generator(device=dev).manual_seed(n)
-        x = torch.randn(S, L, device=dev, generator=g)
-        w = torch.hann_window(n, device=dev)
-        frames = 1 + L // hop
-        y = torch.empty(S, frames, n // 2 + 1, dtype=torch.complex64, device=dev)
-        ms = timed(lambda: plan.exec_stft(x.data_ptr(), y.data_ptr(), n, S, L, hop, True, w.data_ptr(), sh))
-        fb = S * frames * (4 * n + 8 * (n // 2 + 1))
-        # the first 8 frames depend only on a prefix (left reflect padding + 8 hops + one frame)
-        ref = torch.stft(x[:1, :16 * n].double(), n, hop_length=hop, window=w.double(), return_complex=True)[..., :8]
-        got = y[:1, :8].transpose(-1, -2).to(torch.complex128)
-        err = float((torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)).item())
-        # inverse STFT of the same spectrum back to the 4 signals; bytes = spectrum read + signal
-        # written (the two-kernel path also writes and reads every frame once in between)
-        xb = torch.empty(S, L, device=dev)
-        ms_i = timed(lambda: plan.exec_istft(y.data_ptr(), xb.data_ptr(), n, S, frames, hop, True, w.data_ptr(), L,
-                                             1.0, sh))
-        ib = S * frames * 8 * (n // 2 + 1) + 4 * S * L
-        rt = float((torch.linalg.vector_norm(xb - x) / torch.linalg.vector_norm(x)).item())
-        out["stft"][f"n{n}_hop{hop}_S{S}_L{L}"] = {"frame_gbs": round(fb / ms / 1e6, 1),
-                                                    "frac": round(fb / ms / 1e6 / peak, 4), "rel_l2": err,
-                                                    "frames": S * frames,
-                                                    "istft_gbs": round(ib / ms_i / 1e6, 1),
-                                                    "istft_ms": round(ms_i, 4), "round_trip_rel_l2": rt}
-        del x, y, xb
-    # ---- real transforms: R2C forward and its adjoint (weighted C2R), batch 1024
-    for n in (128, 1024, 4096, 8192, 400, 1000):
-        b = 1024
-        g = torch.Generator(device=dev).manual_seed(n)
-        x = torch.rand(b, n, device=dev, generator=g) * 2 - 1
-        X = torch.empty(b, n // 2 + 1, dtype=torch.complex64, device=dev)
-        gx = torch.empty_like(x)
-        plan = bfly.plan_for(dev, n, "real")
-        byts = (8 * n + 8) * b
-        ms_f = timed(lambda: plan.exec_r2c(x.data_ptr(), X.data_ptr(), n, b, 1.0, 1.0, sh))
-        ms_b = timed(lambda: plan.exec_c2r(X.data_ptr(), gx.data_ptr(), n, b, 1.0, 0.5, 1.0, sh))
-        idx = O.sample_batches(b, 4)
-        ref = np.fft.rfft(x[idx].cpu().numpy().astype(np.float64), axis=-1)
-        out["real_fwd_adjoint"][f"n{n}_b{b}"] = {
-            "r2c_gbs": round(byts / (ms_f / 1e3) / 1e9, 1), "adjoint_c2r_gbs": round(byts / (ms_b / 1e3) / 1e9, 1),
-            "r2c_rel_l2": O.rel_l2_rows(X[idx].cpu().numpy(), ref)}
-        del x, X, gx
-    torch.cuda.synchronize()
-    return out
+        for n in (8192, 16384, 32768, 65536):
+            b = (1 << 26) // n
+            g = torch.Generator(device=self.dev).manual_seed(11)
+            x = torch.randn(b, n, dtype=torch.complex64, device=self.dev, generator=g)
+            y = torch.empty_like(x)
+            z = torch.empty_like(x)
+            plan = bfly.plan_for(self.dev, n)
+            byts = 16 * n * b
+            ms_f = self.timed(lambda: self.check(plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh), "fwd"))
+            ms_b = self.timed(lambda: self.check(plan.exec_c2c(y.data_ptr(), z.data_ptr(), n, b, 1, 1.0, sh), "bwd"))
+            res[n] = [round(self.gbs(byts, ms_f), 1), round(self.gbs(byts, ms_b), 1),
+                      float(f"{self.err(y, x, rows=2):.3g}"), float(f"{self.err(z, y, inverse=True, rows=2):.3g}")]
+            del x, y, z
+        emit({"sub": "long_fwd_bwd", "unit": UNIT, "cols": ["fwd_gbs", "bwd_gbs", "fwd_rel_l2", "bwd_rel_l2"],
+              "rows": {f"n{n}_b{(1 << 26) // n}": v for n, v in res.items()}})
+        self.summary["long_fwd_bwd_frac"] = {str(n): [round(v[0] / peak, 3), round(v[1] / peak, 3)] for n, v in res.items()}
+
+    # -- 2-D and strided transforms
+    def c2c_2d(self):
+        torch, sh, peak = self.torch, self.sh, self.peak
+        import bfly
+        out = {}
+        for ny, nx in ((256, 256), (512, 512), (1024, 1024), (2048, 2048), (1024, 128), (128, 1024)):
+            b = (1 << 26) // (ny * nx)
+            g = torch.Generator(device=self.dev).manual_seed(ny + nx)
+            x = torch.randn(b, ny, nx, dtype=torch.complex64, device=self.dev, generator=g)
+            y = torch.empty_like(x)
+            plan = bfly.plan_for(self.dev, nx)
+            ms = self.timed(lambda: self.check(plan.exec_c2c_2d(x.data_ptr(), y.data_ptr(), ny, nx, b, -1, 1.0, sh), "2d"))
+            ref = np.fft.fft2(x[:1].cpu().numpy().astype(np.complex128)).reshape(1, -1)
+            e = rel_l2_rows(y[:1].cpu().numpy().reshape(1, -1), ref)
+            out[f"{ny}x{nx}_b{b}"] = [round(self.gbs(16 * ny * nx * b, ms), 1), float(f"{e:.3g}")]
+            del x, y
+        for n, outer, inner in ((1024, 64, 1024), (256, 1024, 256)):
+            g = torch.Generator(device=self.dev).manual_seed(n + inner)
+            x = torch.randn(outer, n, inner, dtype=torch.complex64, device=self.dev, generator=g)
+            y = torch.empty_like(x)
+            plan = bfly.plan_for(self.dev, n)
+            ms = self.timed(lambda: self.check(plan.exec_c2c_axis(x.data_ptr(), y.data_ptr(), n, outer, inner, -1, 1.0, sh), "axis"))
+            ref = np.fft.fft(x[:1].cpu().numpy().astype(np.complex128), axis=1)
+            e = float(np.linalg.norm(y[:1].cpu().numpy() - ref) / np.linalg.norm(ref))
+            out[f"axis_n{n}_outer{outer}_inner{inner}"] = [round(self.gbs(16 * n * outer * inner, ms), 1), float(f"{e:.3g}")]
+            del x, y
+        emit({"sub": "c2c_2d", "unit": UNIT, "cols": ["gbs", "rel_l2"], "rows": out,
+              "note": "2-D = row pass + column pass (two HBM round trips) scored on 16 bytes per point"})
+
+    # -- non-power-of-two lengths
+    def any_length(self):
+        torch, sh = self.torch, self.sh
+        import bfly
+        out = {}
+        for n in (1536, 1920, 6144, 360, 1000, 3000, 6561, 12000, 1001, 1003, 8191):
+            b = (1 << 25) // n
+            g = torch.Generator(device=self.dev).manual_seed(n)
+            x = torch.randn(b, n, dtype=torch.complex64, device=self.dev, generator=g)
+            y = torch.empty_like(x)
+            plan = bfly.plan_for(self.dev, n)
+            ms = self.timed(lambda: self.check(plan.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh), "c2c"))
+            out[f"n{n}_b{b}"] = [round(self.gbs(16 * n * b, ms), 1), float(f"{self.err(y, x):.3g}")]
+            del x, y
+        emit({"sub": "c2c_any_length", "unit": UNIT, "cols": ["gbs", "rel_l2"], "rows": out})
+
+    # -- STFT / inverse STFT, 4 signals of 2^24 samples, centred, Hann
+    def stft(self):
+        torch, sh = self.torch, self.sh
+        import bfly
+        out = {}
+        plan = bfly.plan_for(self.dev, 1024, "real")
+        for n, hop in ((256, 64), (1024, 256), (4096, 1024), (400, 160)):
+            L, S = 1 << 24, 4
+            g = torch.Generator(device=self.dev).manual_seed(n)
+            x = torch.randn(S, L, device=self.dev, generator=g)
+            w = torch.hann_window(n, device=self.dev)
+            frames = 1 + L // hop
+            y = torch.empty(S, frames, n // 2 + 1, dtype=torch.complex64, device=self.dev)
+            ms = self.timed(lambda: self.check(plan.exec_stft(x.data_ptr(), y.data_ptr(), n, S, L, hop, True, w.data_ptr(), sh)[0], "stft"))
+            fb = S * frames * (4 * n + 8 * (n // 2 + 1))
+            ref = torch.stft(x[:1, :16 * n].double(), n, hop_length=hop, window=w.double(), return_complex=True)[..., :8]
+            got = y[:1, :8].transpose(-1, -2).to(torch.complex128)
+            e = float((torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)).item())
+            xb = torch.empty(S, L, device=self.dev)
+            ms_i = self.timed(lambda: self.check(plan.exec_istft(y.data_ptr(), xb.data_ptr(), n, S, frames, hop, True,
+                                                                 w.data_ptr(), L, 1.0, sh), "istft"))
+            ib = S * frames * 8 * (n // 2 + 1) + 4 * S * L
+            rt = float((torch.linalg.vector_norm(xb - x) / torch.linalg.vector_norm(x)).item())
+            out[f"n{n}_hop{hop}"] = [round(self.gbs(fb, ms), 1), round(ms, 3), float(f"{e:.3g}"),
+                                     round(self.gbs(ib, ms_i), 1), round(ms_i, 3), float(f"{rt:.3g}")]
+            del x, y, xb
+        emit({"sub": "stft", "unit": UNIT, "signals": "4 x 2^24 samples, centred, Hann",
+              "cols": ["stft_frame_gbs", "stft_ms", "stft_rel_l2_vs_torch_f64", "istft_gbs", "istft_ms",
+                       "round_trip_rel_l2"], "rows": out})
 
 
+# ------------------------------------------------------------------ our arm
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
@@ -476,7 +627,6 @@ def run_ours(args):
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
     import bfly
-    import oracle.fft_oracle as O
 
     ctx = bfly.Context()
     rc = ctx.init(device=dev.index)
@@ -493,15 +643,18 @@ def run_ours(args):
             g = torch.Generator(device=dev).manual_seed(grid_seed(n, b))
             x = torch.randn(b, n, dtype=torch.complex64, device=dev, generator=g)
             pts.append((n, b, x, torch.empty_like(x)))
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter()
     for n, b, x, y in pts:   # builds twiddle tables outside any capture
         assert plan.prepare(n, b) == 0
+    plan_setup_us = (time.perf_counter() - t_setup) * 1e6
 
     def check(tag):
         worst = 0.0
         for n, b, x, y in pts:
-            rows = O.sample_batches(b, 2)
+            rows = sample_rows(b, 2)
             ref = np.fft.fft(x[rows].cpu().numpy().astype(np.complex128), axis=-1)
-            worst = max(worst, O.rel_l2_rows(y[rows].cpu().numpy(), ref))
+            worst = max(worst, rel_l2_rows(y[rows].cpu().numpy(), ref))
         assert worst <= 1e-6, f"{tag} parity check failed: rel L2 {worst}"
         return worst
 
@@ -511,7 +664,7 @@ def run_ours(args):
             if r:
                 raise RuntimeError(f"exec_c2c({n},{b}) = {r}")
 
-    # the product path: one ragged persistent launch over all 49 requests
+    # the product path: one ragged launch over all 49 requests
     ragged = plan.make_ragged((x.data_ptr(), y.data_ptr(), n, b, -1, 1.0) for n, b, x, y in pts)
 
     def ragged_step():
@@ -519,7 +672,7 @@ def run_ours(args):
         if r:
             raise RuntimeError(f"ragged exec = {r}")
 
-    # parity spot checks of both paths before timing
+    # parity spot checks of both paths before timing (FP64 numpy FFT on sampled rows)
     with torch.cuda.stream(stream):
         per_point()
     stream.synchronize()
@@ -550,6 +703,14 @@ def run_ours(args):
         e1.record(stream)
         e1.synchronize()
         if sampler:
+            # the timed region lasts a few ms, shorter than one NVML sample interval allows to
+            # resolve well: keep sampling while the same step repeats for ~0.5 s more
+            sampler.in_region = len(sampler.samples)
+            t_end = time.perf_counter() + 0.5
+            while time.perf_counter() < t_end:
+                for _ in range(50):
+                    fn()
+                stream.synchronize()
             sampler.__exit__(None, None, None)
         t = e0.elapsed_time(e1) / steps
         torch.cuda.synchronize()
@@ -583,50 +744,73 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     achieved = grid_bytes() / (ms / 1e3) / 1e9
 
-    # e2e through the C ABI with pinned host buffers: H2D + kernel + D2H per grid point
+    # e2e through the C ABI with pinned host buffers: the whole grid in one
+    # bfly_plan_run_c2c_many call (H2D, kernels and D2H of different points overlap)
     host = []
     for (nn, bb, x, y) in pts:
         hx = torch.empty((bb, 2 * nn), dtype=torch.float32, pin_memory=True)
         hx.copy_(torch.view_as_real(x).reshape(bb, 2 * nn).cpu())
         hy = torch.empty_like(hx).pin_memory()
-        host.append((nn, bb, hx.numpy(), hy.numpy()))
-    e2e_steps = max(1, min(args.steps, 5))
-    # (1) the whole grid in one bfly_plan_run_c2c_many call (copies of different points overlap);
-    # (2) the reference's per-call pattern, bfly_plan_run_c2c once per point (reported beside it)
-    many = [(hx, hy, nn, bb) for nn, bb, hx, hy in host]
-    assert plan.run_many(many) == 0   # warm-up: device buffers grow to the whole grid
-    for nn, bb, hx, hy in host:
-        assert plan.run(hx, hy, nn, bb) == 0
+        host.append((nn, bb, hx, hy))
+    many = [(hx.numpy(), hy.numpy(), nn, bb) for nn, bb, hx, hy in host]
+    t0 = time.perf_counter()
+    assert plan.run_many(many) == 0   # first use: device buffers grow to the whole grid
+    first_use_us = (time.perf_counter() - t0) * 1e6
+    e2e_steps = max(3, min(args.steps, 5))
 
     def e2e_time(step):
         if dist:
             dist.barrier()
-        t0 = time.perf_counter()
+        walls = []
         for _ in range(e2e_steps):
+            t0 = time.perf_counter()
             step()
-        el = (time.perf_counter() - t0) / e2e_steps
+            walls.append(time.perf_counter() - t0)
+        el = statistics.mean(walls)
         if dist:
             t = torch.tensor([el], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             el = t.item()
-        return el
+        return el, walls
 
     def step_many():
         r = plan.run_many(many)
         if r:
             raise RuntimeError(f"run_many = {r}")
 
-    def step_per_call():
-        for nn, bb, hx, hy in host:
-            r = plan.run(hx, hy, nn, bb)
-            if r:
-                raise RuntimeError(f"run({nn},{bb}) = {r}")
-
-    e2e_s = e2e_time(step_many)
-    per_call_s = e2e_time(step_per_call)
+    e2e_s, walls = e2e_time(step_many)
+    # result check of the host round trip on sampled rows
+    for nn, bb, hx, hy in host[::8]:
+        rows = sample_rows(bb, 2)
+        xs = hx.numpy()[rows].view(np.complex64).astype(np.complex128)
+        assert rel_l2_rows(hy.numpy()[rows].view(np.complex64), np.fft.fft(xs, axis=-1)) <= 1e-6
+    # event spans of the same bytes, one phase at a time (no overlap): upload of every input,
+    # the device chain (the ragged launch), download of every output
+    spans = {"h2d": [], "device_chain": [], "d2h": []}
+    for _ in range(e2e_steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            for (nn, bb, hx, hy), (_, _, x, y) in zip(host, pts):
+                torch.view_as_real(x).reshape(bb, 2 * nn).copy_(hx, non_blocking=True)
+            ev[1].record(stream)
+            ragged_step()
+            ev[2].record(stream)
+            for (nn, bb, hx, hy), (_, _, x, y) in zip(host, pts):
+                hy.copy_(torch.view_as_real(y).reshape(bb, 2 * nn), non_blocking=True)
+            ev[3].record(stream)
+        ev[3].synchronize()
+        spans["h2d"].append(ev[0].elapsed_time(ev[1]) * 1e3)
+        spans["device_chain"].append(ev[1].elapsed_time(ev[2]) * 1e3)
+        spans["d2h"].append(ev[2].elapsed_time(ev[3]) * 1e3)
     h2d = sum(8 * nn * bb for nn, bb, _, _ in host)
     e2e_value = grid_bytes() * world / e2e_s / 1e9
-    per_call_value = grid_bytes() * world / per_call_s / 1e9
+    scopes = {"plan_setup_us": round(plan_setup_us, 1), "first_use_us": round(first_use_us, 1),
+              "host_end_to_end_mean_us": round(statistics.mean(walls) * 1e6, 1),
+              "host_end_to_end_min_us": round(min(walls) * 1e6, 1),
+              "h2d_us": round(min(spans["h2d"]), 1), "device_chain_us": round(min(spans["device_chain"]), 1),
+              "d2h_us": round(min(spans["d2h"]), 1), "reps": e2e_steps,
+              "note": "spans: min over reps, phases run one after another; end_to_end overlaps them"}
     info = ragged.info()
     ragged.close()
     del graph
@@ -637,13 +821,26 @@ def run_ours(args):
     if rank != 0:
         return 0
 
-    extras = extra_measurements(dev, stream) if world == 1 and not args.no_extras else None
+    summary = {"sub": "summary"}
+    if world == 1 and not args.no_extras:
+        subs = Subs(dev, stream, ctx, plan)
+        for part in (subs.c2c_2d, subs.any_length, subs.stft, subs.long_fwd_bwd, subs.real_transforms,
+                     subs.ragged_mix, subs.grid_points):
+            part()
+        torch.cuda.synchronize()
+        summary.update(subs.summary)
     cpu = None
     if world == 1:
+        std = cpu_stdlib()
+        emit(std)
+        c1 = std["rows"][0]
+        summary["cpu_stdlib_cfg1_us"] = {"numpy_mean": c1[2], "numpy_min": c1[3], "torch_mean": c1[4],
+                                         "torch_min": c1[5], "numpy": std["numpy"],
+                                         "torch_threads": std["torch_threads"]}
         threads = os.cpu_count() or 1
         gbs, dt, nb, kind, desc = cpu_reference_sample(256, 10.0, threads)
-        cpu = {"value": round(gbs, 4), "unit": UNIT, "cores": threads, "kind": kind, "sample": desc,
-               "stdlib_numpy_1core_gbs": round(stdlib_numpy_sample(3.0), 4)}
+        cpu = {"value": round(gbs, 4), "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
+    tr, tw = grid_traffic()
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 5),
@@ -651,31 +848,27 @@ def run_ours(args):
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "points": len(pts), "bytes_per_step": total_bytes,
                    "l2": "355 MB in + 355 MB out per step > 126 MB L2; no flush",
-                   "launch": "one ragged launch (k_ragged_flat, one tile per CTA) per step",
-                   "parallelism": f"batch-sharded replicas x{world}", "candidate": plan.candidate_id,
-                   "ragged": info, "parity_rel_l2_max": worst},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": dominant_traffic(),
-                     "kernel": "k_ragged_flat over the 49-point grid", "peak_kind": peak_kind,
-                     "launch_us": round(ms * 1e3, 3), "algorithmic_bytes": grid_bytes()},
-        "per_point_graph": {"value": round(per_point_gbs, 2), "unit": UNIT,
-                            "ms_per_step": round(ms_graph, 5), "launches_per_step": len(pts)},
-        "largest_launch": {"kernel": "k_c2c<4096,16,1,fwd> N=4096 batch=4096",
-                           "achieved": round(dom_bytes / (dom_ms / 1e3) / 1e9, 2),
+                   "launch": "one k_ragged_flat launch per step", "tiles": info["tiles"],
+                   "parallelism": f"batch-sharded replicas x{world}", "parity_rel_l2_max": float(f"{worst:.3g}")},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4),
+                     "traffic": (tr + tw) if tr is not None else None, "traffic_read": tr,
+                     "traffic_note": "ncu dram bytes inside the launch; writes left dirty in L2 drain after it",
+                     "kernel": "k_ragged_flat", "peak_kind": peak_kind, "algorithmic_bytes": grid_bytes()},
+        "per_point_graph": {"value": round(per_point_gbs, 1), "launches_per_step": len(pts)},
+        "largest_launch": {"kernel": "k_c2c N=4096 batch=4096",
                            "frac": round(dom_bytes / (dom_ms / 1e3) / 1e9 / peak, 4),
-                           "launch_us": round(dom_ms * 1e3, 3)},
-        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": h2d,
-                "path": "bfly_plan_run_c2c_many over the 49 grid points, pinned host buffers",
-                "per_call": {"value": round(per_call_value, 3), "unit": UNIT,
-                             "path": "bfly_plan_run_c2c once per grid point (the reference's call pattern)"}},
+                           "launch_us": round(dom_ms * 1e3, 2)},
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": h2d, "path": "bfly_plan_run_c2c_many, pinned host buffers",
+                "scopes": scopes},
         "gpu_launches": args.steps,
         "clocks": clocks.summary() if clocks else None,
         "cpu_baseline": cpu,
     }
-    if extras:
-        line.update(extras)
-    print(json.dumps(line), flush=True)
+    if len(summary) > 1:
+        emit(summary)
+    emit(line)
     return 0
 
 
@@ -774,7 +967,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default=None, help="kind:n:batch (see run_case), launch only that kernel (for ncu)")
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--no-extras", action="store_true", help="skip the split-BF16 / fwd+bwd sub-measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the sub-measurements beside the headline")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)

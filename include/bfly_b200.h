@@ -242,10 +242,13 @@ void bfly_ragged_destroy(bfly_ragged* ragged);
  * Its workspace is a fixed 32 MiB array in the library's device image (every GPU that loads
  * the library keeps it until exit), so n * batch must be <= 4,194,304 complex values; larger
  * requests return -12 before any GPU work.  No plan or context is needed: it runs on the
- * current device.  The first call on a device looks up the array addresses, builds its twiddle
- * tables on `stream` and waits for that stream once; make that first call before any stream
- * capture.  All calls share the one workspace: calls that overlap on the GPU race.
- * Status: 0, -8 shape/direction, -10 null pointer, -12 too large, -1 runtime, -5 launch. */
+ * current device.  The first call on a device looks up the array addresses, loads every kernel
+ * variant it can launch, builds its twiddle tables on `stream` and waits for that stream once;
+ * make that first call before any stream capture (a first call on a stream that is being
+ * captured returns -13 and leaves the capture untouched).  All calls share the one workspace:
+ * calls that overlap on the GPU race.
+ * Status: 0, -8 shape/direction, -10 null pointer, -12 too large, -13 first call on a capturing
+ * stream, -1 runtime, -5 launch. */
 int bfly_exec_c2c_long_noalloc(const void* d_in, void* d_out, uint32_t n, uint64_t batch,
                                int direction, float scale, void* stream);
 

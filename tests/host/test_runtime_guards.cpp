@@ -439,6 +439,10 @@ int main(int argc, char** argv) {
         CHECK(plan->execC2C2D(d, d, 48, 64, 1, -1, 1.f, nullptr) == -8);      // ny not a power of two
         CHECK(plan->execC2C2D(d, d, 32, 9001, 1, -1, 1.f, nullptr) == -8);    // nx beyond every row kernel
         CHECK(plan->execC2C2D(d, d, 4096, 64, 1u << 20, -1, 1.f, nullptr) == -8);   // batch*ny > 2^32-1
+        // batch * ny wraps to a small value in 64 bits (2^52 * 4096 = 2^64 -> 0; +1 row -> 4096)
+        CHECK(plan->execC2C2D(d, d, 4096, 64, (1ull << 52) + 1, -1, 1.f, nullptr) == -8);
+        CHECK(plan->execR2C2D(d, d, 4096, 64, (1ull << 52) + 1, 1.f, nullptr) == -8);
+        CHECK(plan->execC2R2D(d, d, 4096, 64, (1ull << 52) + 1, 1.f, nullptr) == -8);
         CHECK(plan->execC2CAxis(d, d, 32, 0, 3, -1, 1.f, nullptr) == -8);
         CHECK(plan->execC2CAxis(d, d, 32, 1, 0, -1, 1.f, nullptr) == -8);
         CHECK(plan->execC2CAxis(d, d, 8192, 1, 3, -1, 1.f, nullptr) == -8);   // strided n above 4096

@@ -67,3 +67,16 @@ def test_pattern_and_sampling_match_oracle(lib):
         buf = (ctypes.c_uint32 * 16)()
         cnt = lib.bfly_sample_batches(batch, want, buf, 16)
         assert list(buf[:cnt]) == O.sample_batches(batch, want)
+
+
+def test_noalloc_long_size_guard_without_gpu(lib):
+    """The allocation-free long C2C rejects oversize requests before any CUDA call, including a
+    batch whose product with n wraps in 64 bits (65536 * (2^48 + 1) = 65536 mod 2^64)."""
+    import ctypes as C
+    p = C.c_void_p(16)   # never dereferenced: every call is rejected first
+    f = lib.bfly_exec_c2c_long_noalloc
+    assert f(p, p, 65536, (1 << 48) + 1, -1, 1.0, None) == -12
+    assert f(p, p, 65536, 65, -1, 1.0, None) == -12
+    assert f(p, p, 8192, 513, 1, 1.0, None) == -12
+    assert f(p, p, 8192, 0, -1, 1.0, None) == -8
+    assert f(None, p, 8192, 1, -1, 1.0, None) == -10

@@ -98,3 +98,40 @@ def test_rfft_grad_vs_fp64_finite_differences(cuda):
         xm = x.copy(); xm[i, j] -= h
         fd = (loss64(xp) - loss64(xm)) / (2 * h)
         assert abs(grad[i, j] - fd) <= 1e-3 * max(1.0, abs(fd)), (i, j, grad[i, j], fd)
+
+
+@pytest.mark.parametrize("n,batch,seed", [(64, 2, 3), (1024, 2, 4), (8192, 2, 11), (65536, 1, 11)])
+@pytest.mark.parametrize("op", ["fft", "ifft"])
+def test_c2c_grad_vs_fp64_finite_differences(cuda, n, batch, seed, op):
+    """Loss = sum(w * |F(x)|^2) with F = fft or ifft on complex x (the long lengths under the
+    long-transform loss: x ~ N(0,1), w ~ U(0,1), seeded): the conjugate-FFT adjoint against FP64
+    central differences of the real and imaginary part of sampled entries.  torch's gradient of
+    a real loss in a complex input is dL/dRe + i dL/dIm.  The loss is quadratic, so the central
+    difference is exact up to FP64 rounding."""
+    torch = _torch()
+    import bfly
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((batch, n)) + 1j * rng.standard_normal((batch, n))
+    x = x.astype(np.complex64).astype(np.complex128)
+    w = rng.uniform(0, 1, (batch, n))
+    f64 = np.fft.fft if op == "fft" else np.fft.ifft
+
+    def loss64(xx):
+        return float((w * np.abs(f64(xx, axis=-1)) ** 2).sum())
+
+    xt = torch.tensor(x, dtype=torch.complex64, device=cuda, requires_grad=True)
+    wt = torch.tensor(w, dtype=torch.float32, device=cuda)
+    (wt * getattr(bfly, op)(xt).abs() ** 2).sum().backward()
+    grad = xt.grad.cpu().numpy().astype(np.complex128)
+    idx = [(0, 0), (0, 1), (0, n // 2), (batch - 1, n // 3), (batch - 1, n - 1)]
+    h = 1e-3
+    got, want = [], []
+    for (i, j) in idx:
+        for unit in (1.0, 1j):
+            xp = x.copy(); xp[i, j] += h * unit
+            xm = x.copy(); xm[i, j] -= h * unit
+            want.append((loss64(xp) - loss64(xm)) / (2 * h))
+            got.append(grad[i, j].real if unit == 1.0 else grad[i, j].imag)
+    got, want = np.array(got), np.array(want)
+    rel = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert rel <= 1e-5, (op, n, rel)
