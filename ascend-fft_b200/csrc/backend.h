@@ -78,6 +78,18 @@ int launchLongB(const void* in, void* out, uint32_t n1, uint32_t n2, uint64_t ba
 // memory, so that later launches neither load device code nor set kernel attributes.
 int prepareLongKernels();
 
+// Long C2C as one persistent cooperative launch of the four-step schedule, the intermediate
+// kept in a ring of longRingSlots() slots of `slotRows` rows each (L2-resident): `ring` holds
+// min(slots, ceil(batch / slotRows)) * slotRows * n complex values, `counters` 2 * slots
+// unsigned values (zeroed by the launch on `stream`).  Tables as for the four-step kernels.
+bool hasLongRing(uint32_t n);
+int longRingSlots();
+uint32_t longRingSlotRows(uint32_t n, uint64_t batch, size_t slotBytes);
+int launchLongRing(const void* in, void* out, void* ring, uint32_t slotRows, uint32_t n, uint64_t batch,
+                   bool inverse, float scale, const void* tw1, const void* tw2, const void* tlo, const void* thi,
+                   void* counters, void* stream);
+int longRingStatus(unsigned* status, bool clear);   // nonzero *status: a bounded wait ran out
+
 // Single-pass long C2C: one thread-block cluster per row, transpose through distributed
 // shared memory (n in 8192..65536; tw1 = Stockham (n/256, 16), tw2 = Stockham (256, 16)).
 // `cta` threads per CTA (256, or 512 for n >= 16384) sets the cluster size n / (16 * cta).
@@ -235,8 +247,11 @@ int raggedStatus(unsigned* status, bool clear);
 bool hasTensorVariant(uint32_t n, int split);
 size_t tensorTableBytes(int split);                            // split DFT-16 operand
 int buildTensorTable(void* table, int split, void* stream);    // FP64 on the device
+// twTc: twiddles of the tensor-core passes after the first, by operand row (FP64 on the device).
+size_t tensorTwiddleCount(uint32_t n);
+int buildTensorTwiddles(void* tw, uint32_t n, void* stream);
 int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
-                    const void* tw, const void* table, int split, void* stream);
+                    const void* tw, const void* twTc, const void* table, int split, void* stream);
 int tensorStatus(unsigned* status, bool clear);
 
 }  // namespace backend

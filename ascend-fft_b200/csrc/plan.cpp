@@ -40,6 +40,13 @@ constexpr uint32_t kMinN = 32;        // two passes of radix <= 16
 constexpr uint32_t kMaxSinglePass = 16384;
 constexpr uint32_t kMaxN = 65536;
 
+// Ring slots of the "ring" schedule (k_long_ring.cu): BFLY_LONG_RING_MB megabytes, default 8.
+size_t longRingSlotBytes() {
+    const char* env = std::getenv("BFLY_LONG_RING_MB");
+    const long mb = env ? std::strtol(env, nullptr, 10) : 8;
+    return (size_t)(mb >= 1 && mb <= 1024 ? mb : 8) << 20;
+}
+
 std::string slurp(const std::string& path) {
     std::ifstream f(path, std::ios::binary);
     if (!f) throw std::runtime_error("cannot read configuration: " + path);
@@ -167,7 +174,7 @@ DesignSpace DesignSpace::load(const std::string& path) {
     stringAxis(l, "in", &sp.layoutsIn, {"interleaved", "planar"});
     stringAxis(l, "out", &sp.layoutsOut, {"interleaved", "planar"});
     stringAxis(f, "precision", &sp.precisions, {"fp32", "split_bf16"});
-    stringAxis(f, "schedule", &sp.schedules, {"stockham", "four_step", "cluster"});
+    stringAxis(f, "schedule", &sp.schedules, {"stockham", "four_step", "cluster", "ring"});
     return sp;
 }
 
@@ -209,6 +216,7 @@ Metric estimate(const Hardware& hw, const Candidate& c, uint32_t n, uint32_t bat
     double us = 2.5 + hbmUs * (1.0 + 0.04 * std::max(0, passes - 2));
     if (c.f.schedule == "four_step") us = 3.0 + 2.0 * hbmUs;
     if (c.f.schedule == "cluster") us = 3.0 + 1.3 * hbmUs;
+    if (c.f.schedule == "ring") us = 3.0 + 2.4 * hbmUs;   // measured 0.84-0.97x of four_step
     if (c.a.ctaThreads < 256) us *= 1.02;
     m.etaUs = us;
     return m;
@@ -283,6 +291,11 @@ std::vector<Candidate> enumerate(const DesignSpace& sp, const Hardware& hw, uint
             else if (!backend::hasLongCluster(n, cta))
                 infeasible("no cluster kernel for this (n, cta_threads): 256 threads per CTA, or 512 for n >= 16384");
             else c.state = State::Unverified;
+        } else if (sched == "ring") {
+            if (!backend::hasLongRing(n)) infeasible("ring schedule serves n = 8192 .. 65536");
+            else if (radix != backend::longE() || cta != 256)
+                infeasible("ring kernels use radix 16 and 256-thread CTAs");
+            else c.state = State::Unverified;
         } else if (sched == "four_step") {
             uint32_t n1 = 0, n2 = 0;
             backend::longSplit(n, &n1, &n2);
@@ -334,7 +347,8 @@ static bool lowerable(const Candidate& c, const Hardware& hw) {
            (c.p.radix == 8 || c.p.radix == 16) && c.l.contiguous &&
            c.l.in == Layout::Interleaved && c.l.out == Layout::Interleaved &&
            c.f.precision == "fp32" &&
-           (c.f.schedule == "stockham" || c.f.schedule == "four_step" || c.f.schedule == "cluster") &&
+           (c.f.schedule == "stockham" || c.f.schedule == "four_step" || c.f.schedule == "cluster" ||
+            c.f.schedule == "ring") &&
            (c.a.ctaThreads == 128 || c.a.ctaThreads == 256 || c.a.ctaThreads == 512 ||
             c.a.ctaThreads == 1024);
 }
@@ -354,6 +368,8 @@ struct Plan::Impl {
     void* devOut = nullptr;
     void* devWork = nullptr;
     size_t devInCap = 0, devOutCap = 0, devWorkCap = 0;
+    void* devRingCtr = nullptr;   // item counters of the L2-ring long C2C
+    size_t devRingCtrCap = 0;
     backend::Timer* timer = nullptr;
     void* aux[2] = {nullptr, nullptr};   // upload / download streams of the pipelined host round trip
     void* ev[2] = {nullptr, nullptr};    // chunk uploaded / chunk transformed
@@ -367,6 +383,7 @@ struct Plan::Impl {
     void* evStage[2] = {nullptr, nullptr};
     void* evOut[2] = {nullptr, nullptr};
     void* tcTable[4] = {nullptr, nullptr, nullptr, nullptr};   // split DFT-16 operand per term count
+    std::map<uint32_t, void*> twTc;                            // n -> tensor-core pass twiddles by row
     struct Chirp {
         void* chirp = nullptr;   // c[j] = exp(-i*pi*j^2/n), j < n
         void* filt = nullptr;    // FFT_M of the padded conj(c) sequence, / M
@@ -393,6 +410,7 @@ Plan::~Plan() {
     if (impl_->devIn) backend::release(impl_->devIn);
     if (impl_->devOut) backend::release(impl_->devOut);
     if (impl_->devWork) backend::release(impl_->devWork);
+    if (impl_->devRingCtr) backend::release(impl_->devRingCtr);
     if (impl_->devHalf) backend::release(impl_->devHalf);
     for (int i = 0; i < 2; ++i) {
         if (impl_->pinIn[i]) backend::releaseHost(impl_->pinIn[i]);
@@ -405,6 +423,8 @@ Plan::~Plan() {
         if (st) backend::streamDestroy(st);
     for (void* e : impl_->ev)
         if (e) backend::eventDestroy(e);
+    for (auto& kv : impl_->twTc)
+        if (kv.second) backend::release(kv.second);
     for (void* t : impl_->tcTable)
         if (t) backend::release(t);
     for (auto& kv : impl_->dftSmall)
@@ -480,6 +500,11 @@ int Plan::resolve(int kind, uint32_t n, int* e, int* cta) const {
         if (sched == "stockham" && n <= kMaxSinglePass && backend::hasVariant(backend::kC2C, n, r, c)) {
             *e = r;
             *cta = c;
+            return 0;
+        }
+        if (sched == "ring" && backend::hasLongRing(n)) {
+            *e = -2;
+            *cta = 256;
             return 0;
         }
         if (sched == "cluster" && backend::hasLongCluster(n, 256)) {
@@ -621,8 +646,9 @@ int Plan::prepare(uint32_t n, uint32_t batch) {
     tf_.clear();
     tf_.push_back({Transform::GenTwiddles, "FP64 twiddle tables built on the device, rounded to fp32"});
     tf_.push_back({Transform::LaunchKernel, e > 0 ? "stockham single-pass kernel on the context stream"
-                                            : e < 0 ? "one thread-block cluster per row (on-chip transpose)"
-                                                    : "four-step column + row kernels on the context stream"});
+                                            : e == -1 ? "one thread-block cluster per row (on-chip transpose)"
+                                            : e == -2 ? "one persistent four-step launch, intermediate in an L2 ring"
+                                                      : "four-step column + row kernels on the context stream"});
     return 0;
 }
 
@@ -670,7 +696,7 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
     if (prepareLong(n)) return -2;
     uint32_t n1 = 0, n2 = 0;
     backend::longSplit(n, &n1, &n2);
-    if (e < 0) {
+    if (e == -1) {
         const auto& lt = impl_->twLong[n];
         const int E = backend::longE();
         const int rc = backend::launchLongCluster(dIn, dOut, n, batch, inv, scale, impl_->twC2C[{n1, E}],
@@ -679,12 +705,26 @@ int Plan::execC2CWith(const void* dIn, void* dOut, uint32_t n, uint64_t batch, i
         if (rc != backend::kLongClusterUnaligned) return -5;
         // an input the tensor map cannot address: the four-step kernels below take any float2 pointer
     }
+    const auto& lt = impl_->twLong[n];
+    const int E = backend::longE();
+    if (e == -2 && !work) {
+        // one persistent launch, the intermediate in an L2-resident ring of three row slots
+        const uint32_t slotRows = backend::longRingSlotRows(n, batch, longRingSlotBytes());
+        const uint64_t chunks = (batch + slotRows - 1) / slotRows;
+        const size_t ringBytes = (size_t)std::min<uint64_t>(chunks, (uint64_t)backend::longRingSlots()) * slotRows * n * 8;
+        if (ensureBuf(&impl_->devWork, &impl_->devWorkCap, ringBytes) ||
+            ensureBuf(&impl_->devRingCtr, &impl_->devRingCtrCap, 64))
+            return -3;
+        if (backend::launchLongRing(dIn, dOut, impl_->devWork, slotRows, n, batch, inv, scale,
+                                    impl_->twC2C[{n1, E}], impl_->twC2C[{n2, E}], lt.lo, lt.hi,
+                                    impl_->devRingCtr, s))
+            return -5;
+        return 0;
+    }
     if (!work) {
         if (ensureBuf(&impl_->devWork, &impl_->devWorkCap, (size_t)n * batch * 8)) return -3;
         work = impl_->devWork;
     }
-    const auto& lt = impl_->twLong[n];
-    const int E = backend::longE();
     if (backend::launchLongA(dIn, work, n1, n2, batch, inv, impl_->twC2C[{n1, E}], lt.lo, lt.hi, s))
         return -5;
     if (backend::launchLongB(work, dOut, n1, n2, batch, inv, scale, impl_->twC2C[{n2, E}], s))
@@ -708,8 +748,20 @@ int Plan::execC2CTensor(const void* dIn, void* dOut, uint32_t n, uint64_t batch,
         }
         table = t;
     }
-    if (backend::launchC2CTensor(dIn, dOut, n, batch, direction > 0, scale, impl_->twC2C[{n, 16}], table,
-                                 splitTerms, stream))
+    if (!impl_->twTc.count(n)) {
+        void* t = nullptr;
+        const size_t count = backend::tensorTwiddleCount(n);
+        if (count) {
+            if (backend::alloc(&t, count * 8)) return -3;
+            if (backend::buildTensorTwiddles(t, n, stream_) || backend::streamSync(stream_)) {
+                backend::release(t);
+                return -2;
+            }
+        }
+        impl_->twTc[n] = t;
+    }
+    if (backend::launchC2CTensor(dIn, dOut, n, batch, direction > 0, scale, impl_->twC2C[{n, 16}],
+                                 impl_->twTc[n], table, splitTerms, stream))
         return -5;
     return 0;
 }
@@ -721,7 +773,10 @@ int Plan::tensorStatus(unsigned* status) {
 
 int Plan::longStatus(unsigned* status) {
     if (!status) return -10;
-    return backend::longClusterStatus(status, true) ? -6 : 0;
+    unsigned ring = 0;
+    if (backend::longClusterStatus(status, true) || backend::longRingStatus(&ring, true)) return -6;
+    *status |= ring ? 2u : 0u;
+    return 0;
 }
 
 // Column pass shared by the 2-D and axis entry points: n-point transforms down `cols`

@@ -135,7 +135,8 @@ class ClockSampler:
 
     def __init__(self, index: int, bus_id: str | None = None):
         self.index, self.bus_id = index, bus_id
-        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.samples, self.times, self.reasons, self.max_mhz = [], [], set(), None
+        self.window = None   # (t0, t1) host time of the timed region
         self._stop = threading.Event()
         self._thread = None
         self._proc = None
@@ -143,14 +144,16 @@ class ClockSampler:
     def _nvml_loop(self, nv, h):
         while not self._stop.is_set():
             try:
+                t = time.perf_counter()
                 self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                self.times.append(t)
                 mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
                 for bit, name in self.REASONS.items():
                     if mask & bit:
                         self.reasons.add(name)
             except Exception:
                 pass
-            time.sleep(0.001)
+            time.sleep(0.0002)
 
     def __enter__(self):
         try:
@@ -187,6 +190,7 @@ class ClockSampler:
             parts = [x.strip() for x in line.split(",")]
             try:
                 self.samples.append(float(parts[0]))
+                self.times.append(time.perf_counter())
                 self.max_mhz = float(parts[1])
             except (ValueError, IndexError):
                 continue
@@ -207,11 +211,17 @@ class ClockSampler:
             self._thread.join(timeout=2)
 
     def summary(self):
+        """Median SM clock over the samples taken inside the timed region (sampling runs from
+        before the warm-up, so a short region still gets the samples that fall in it); the
+        warm-up's samples stand in when none did."""
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+        inside = self.samples
+        if self.window:
+            inside = [c for c, t in zip(self.samples, self.times) if self.window[0] <= t <= self.window[1]]
+        return {"sm_mhz": statistics.median(inside or self.samples), "sm_max_mhz": self.max_mhz,
                 "reasons": sorted(self.reasons), "samples": len(self.samples),
-                "samples_in_timed_region": getattr(self, "in_region", len(self.samples))}
+                "samples_in_timed_region": len(inside) if self.window else len(self.samples)}
 
 
 # ------------------------------------------------------------------ CPU reference
@@ -532,8 +542,15 @@ class Subs:
             ms_b = self.timed(lambda: self.check(plan.exec_c2c(y.data_ptr(), z.data_ptr(), n, b, 1, 1.0, sh), "bwd"))
             res[n] = [round(self.gbs(byts, ms_f), 1), round(self.gbs(byts, ms_b), 1),
                       float(f"{self.err(y, x, rows=2):.3g}"), float(f"{self.err(z, y, inverse=True, rows=2):.3g}")]
+            # the same forward on the ring schedule (one launch, intermediate in L2)
+            ring = self.ctx.make_plan("r16_cta256_shared_fp32_ring", 8192, 1)
+            ms_r = self.timed(lambda: self.check(ring.exec_c2c(x.data_ptr(), z.data_ptr(), n, b, -1, 1.0, sh), "ring"))
+            res[n] += [round(self.gbs(byts, ms_r), 1), float(f"{self.err(z, x, rows=2):.3g}")]
+            ring.close()
             del x, y, z
-        emit({"sub": "long_fwd_bwd", "unit": UNIT, "cols": ["fwd_gbs", "bwd_gbs", "fwd_rel_l2", "bwd_rel_l2"],
+        emit({"sub": "long_fwd_bwd", "unit": UNIT,
+              "cols": ["fwd_gbs", "bwd_gbs", "fwd_rel_l2", "bwd_rel_l2", "ring_fwd_gbs", "ring_rel_l2"],
+              "schedule": "single pass n <= 16384, two-kernel four-step above; ring = one-launch four-step",
               "rows": {f"n{n}_b{(1 << 26) // n}": v for n, v in res.items()}})
         self.summary["long_fwd_bwd_frac"] = {str(n): [round(v[0] / peak, 3), round(v[1] / peak, 3)] for n, v in res.items()}
 
@@ -685,6 +702,10 @@ def run_ours(args):
     worst = max(worst, check("ragged"))
 
     def timed(fn, steps, sample_clocks=False):
+        bus = getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None)
+        sampler = ClockSampler(dev.index, bus) if sample_clocks else None
+        if sampler:   # sampling from before the warm-up: the timed region itself lasts a few ms
+            sampler.__enter__()
         for _ in range(max(3, args.warmup)):
             fn()
         stream.synchronize()
@@ -693,24 +714,14 @@ def run_ours(args):
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        bus = getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None)
-        sampler = ClockSampler(dev.index, bus) if sample_clocks else None
-        if sampler:
-            sampler.__enter__()
+        t0 = time.perf_counter()
         e0.record(stream)
         for _ in range(steps):
             fn()
         e1.record(stream)
         e1.synchronize()
         if sampler:
-            # the timed region lasts a few ms, shorter than one NVML sample interval allows to
-            # resolve well: keep sampling while the same step repeats for ~0.5 s more
-            sampler.in_region = len(sampler.samples)
-            t_end = time.perf_counter() + 0.5
-            while time.perf_counter() < t_end:
-                for _ in range(50):
-                    fn()
-                stream.synchronize()
+            sampler.window = (t0, time.perf_counter())
             sampler.__exit__(None, None, None)
         t = e0.elapsed_time(e1) / steps
         torch.cuda.synchronize()

@@ -380,6 +380,23 @@ int launchLongCluster(const void* in, void* out, uint32_t n, uint64_t batch, boo
 
 int longClusterStatus(unsigned* status, bool) { *status = 0; return 0; }
 
+bool hasLongRing(uint32_t n) { return n == 8192 || n == 16384 || n == 32768 || n == 65536; }
+int longRingSlots() { return 4; }
+uint32_t longRingSlotRows(uint32_t n, uint64_t batch, size_t slotBytes) {
+    uint64_t rows = slotBytes / ((uint64_t)n * 8);
+    if (rows < 1) rows = 1;
+    if (rows > batch) rows = batch;
+    return (uint32_t)rows;
+}
+int launchLongRing(const void* in, void* out, void*, uint32_t, uint32_t n, uint64_t batch, bool inverse, float scale,
+                   const void*, const void*, const void*, const void*, void*, void*) {
+    if (int r = launch()) return r;
+    for (uint64_t b = 0; b < batch; ++b)
+        dft((const float*)in + b * 2 * n, (float*)out + b * 2 * n, n, inverse ? 1 : -1, scale);
+    return 0;
+}
+int longRingStatus(unsigned* status, bool) { *status = 0; return 0; }
+
 int raggedSmemBytes() { return 34816; }
 int raggedGrid(int, int* grid) { *grid = 148 * 2; return 0; }
 int launchRagged(const void* entries, int count, uint64_t, int, void*) {
@@ -408,8 +425,10 @@ bool hasTensorVariant(uint32_t n, int split) {
 }
 size_t tensorTableBytes(int split) { return (size_t)split * 2048; }
 int buildTensorTable(void*, int, void*) { return launch(); }
+size_t tensorTwiddleCount(uint32_t n) { return n >= 256 ? (n >= 4096 ? 2 : 1) * n : 0; }
+int buildTensorTwiddles(void*, uint32_t, void*) { return launch(); }
 int launchC2CTensor(const void* in, void* out, uint32_t n, uint64_t batch, bool inverse, float scale,
-                    const void* tw, const void*, int, void* s) {
+                    const void* tw, const void*, const void*, int, void* s) {
     return launchC2C(in, out, n, batch, inverse, scale, tw, 16, 256, s);
 }
 int tensorStatus(unsigned* status, bool) { *status = 0; return 0; }

@@ -88,7 +88,7 @@ int main(int argc, char** argv) {
                             replaced(spText, "\"radix\": [8, 16]", "\"radix\": [\"8\"]"),
                             replaced(spText, "\"radix\": [8, 16]", "\"radix\": [3]"),
                             replaced(spText, "\"out\": [\"interleaved\", \"planar\"]", "\"out\": [\"bogus\"]"),
-                            replaced(spText, "\"schedule\": [\"stockham\", \"cluster\", \"four_step\"]", "\"schedule\": [\"fast\"]")}) {
+                            replaced(spText, "\"schedule\": [\"stockham\", \"cluster\", \"four_step\", \"ring\"]", "\"schedule\": [\"fast\"]")}) {
         write(badSp, bad);
         CHECK(throws([&] { bfly::DesignSpace::load(badSp); }));
         bfly::Context invalid;
@@ -183,12 +183,12 @@ int main(int argc, char** argv) {
         for (const auto& c : context.enumerate(4096, 524287)) live = live || c.state != bfly::State::Infeasible;
         CHECK(live);
     }
-    {   // long lengths: four-step and cluster feasible, single CTA only up to 16384
-        int fs = 0, cl = 0, sp = 0;
+    {   // long lengths: four-step, ring and cluster feasible, single CTA only up to 16384
+        int fs = 0, cl = 0, rg = 0, sp = 0;
         for (const auto& c : context.enumerate(65536, 4))
             if (c.state != bfly::State::Infeasible)
-                (c.f.schedule == "four_step" ? fs : c.f.schedule == "cluster" ? cl : sp)++;
-        CHECK(fs == 1 && cl == 2 && sp == 0);   // cluster: 256- and 512-thread CTAs
+                (c.f.schedule == "four_step" ? fs : c.f.schedule == "cluster" ? cl : c.f.schedule == "ring" ? rg : sp)++;
+        CHECK(fs == 1 && cl == 2 && rg == 1 && sp == 0);   // cluster: 256- and 512-thread CTAs
         bool single8192 = false;
         for (const auto& c : context.enumerate(8192, 4))
             single8192 = single8192 || (c.state != bfly::State::Infeasible && c.f.schedule == "stockham");
@@ -206,6 +206,7 @@ int main(int argc, char** argv) {
         };
         CHECK(launchLabel("cluster").find("cluster") != std::string::npos);
         CHECK(launchLabel("four_step").find("four-step") != std::string::npos);
+        CHECK(launchLabel("ring").find("L2 ring") != std::string::npos);
         CHECK(fake::allocations == fake::releases && fake::launches > 0);   // plans freed their tables
         fake::allocations = fake::releases = fake::copies = fake::launches = 0;
     }
