@@ -2,6 +2,7 @@
 // kernel-variant resolution and launches of the hand-written sm_100a kernels.
 #include "backend.h"
 #include "fft_kernels.cuh"
+#include "launch.cuh"
 #include "registry.cuh"
 
 #include <atomic>
@@ -161,11 +162,8 @@ int launchC2C(const void* in, void* out, uint32_t n, uint64_t batch, bool invers
     const Entry* x = findEntry(kC2C, n, e, cta, inverse ? 1 : 0);
     if (!x) return (int)cudaErrorInvalidDeviceFunction;
     if (int err = prepareEntry(x)) return err;
-    auto fn = reinterpret_cast<dev::KC2C>(const_cast<void*>(x->fn));
-    fn<<<gridFor(batch, x->rows), x->cta, x->smem, S(stream)>>>(
-        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw),
-        batch, scale);
-    return rc(cudaGetLastError());
+    return rc(launchPdl(x->fn, gridFor(batch, x->rows), x->cta, x->smem, S(stream), static_cast<const float2*>(in),
+                        static_cast<float2*>(out), static_cast<const float2*>(tw), batch, scale));
 }
 
 int launchR2C(const void* in, void* out, uint32_t n, uint64_t batch, const void* tw,
@@ -174,11 +172,9 @@ int launchR2C(const void* in, void* out, uint32_t n, uint64_t batch, const void*
     const Entry* x = findEntry(kR2C, n, e, cta, weighted ? 1 : 0);
     if (!x) return (int)cudaErrorInvalidDeviceFunction;
     if (int err = prepareEntry(x)) return err;
-    auto fn = reinterpret_cast<dev::KR2C>(const_cast<void*>(x->fn));
-    fn<<<gridFor(batch, x->rows), x->cta, x->smem, S(stream)>>>(
-        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw),
-        static_cast<const float2*>(twr), batch, sEdge, sInt);
-    return rc(cudaGetLastError());
+    return rc(launchPdl(x->fn, gridFor(batch, x->rows), x->cta, x->smem, S(stream), static_cast<const float2*>(in),
+                        static_cast<float2*>(out), static_cast<const float2*>(tw), static_cast<const float2*>(twr),
+                        batch, sEdge, sInt));
 }
 
 int launchC2R(const void* in, void* out, uint32_t n, uint64_t batch, const void* tw,
@@ -187,11 +183,9 @@ int launchC2R(const void* in, void* out, uint32_t n, uint64_t batch, const void*
     const Entry* x = findEntry(kC2R, n, e, cta, 0);
     if (!x) return (int)cudaErrorInvalidDeviceFunction;
     if (int err = prepareEntry(x)) return err;
-    auto fn = reinterpret_cast<dev::KC2R>(const_cast<void*>(x->fn));
-    fn<<<gridFor(batch, x->rows), x->cta, x->smem, S(stream)>>>(
-        static_cast<const float2*>(in), static_cast<float2*>(out), static_cast<const float2*>(tw),
-        static_cast<const float2*>(twr), batch, sEdge, sInt, outScale);
-    return rc(cudaGetLastError());
+    return rc(launchPdl(x->fn, gridFor(batch, x->rows), x->cta, x->smem, S(stream), static_cast<const float2*>(in),
+                        static_cast<float2*>(out), static_cast<const float2*>(tw), static_cast<const float2*>(twr),
+                        batch, sEdge, sInt, outScale));
 }
 
 // ------------------------------------------------------------------ four-step

@@ -324,6 +324,17 @@ struct Team {
     }
 };
 
+// ------------------------------------------------------------------ programmatic dependent launch
+// A kernel launched with programmatic stream serialisation may start while the previous kernel
+// on its stream drains: pdl_wait(), before a kernel's first global access, blocks until the
+// previous grid has finished and its writes are visible, so a chain of such launches overlaps
+// only launch latency, never data; pdl_trigger(), just before a CTA's final stores, lets the
+// next kernel launch once every CTA of this grid has reached that point (triggering at entry
+// placed the next grid's CTAs beside this one's and unbalanced one-wave launches).  Without
+// the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ------------------------------------------------------------------ global access helpers
 // Streaming (evict-first) accesses: every input and output element is touched exactly once.
 __device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }

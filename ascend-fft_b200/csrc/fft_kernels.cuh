@@ -39,6 +39,7 @@ k_c2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     constexpr int S = smem_stride<N, E, false>();
     using TM = Team<N, E, INV, sync_kind(T, T * ROWS)>;
     extern __shared__ float2 smem[];
+    pdl_wait();
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
     const uint64_t row = (uint64_t)blockIdx.x * ROWS + rl;
@@ -48,6 +49,7 @@ k_c2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     float2 v[E];
     TM::run(v, smem + rl * S, tw, t, rl,
             [&](int i) { return ok ? ld_stream(src + i) : make_float2(0.f, 0.f); });
+    pdl_trigger();
     if (ok) TM::for_each_out(v, t, [&](int i, float2 x) { st_stream(dst + i, cscale(x, scale)); });
 }
 
@@ -66,6 +68,7 @@ k_r2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     constexpr int S = smem_stride<M, E, false>();
     using TM = Team<M, E, false, sync_kind(T, T * ROWS)>;
     extern __shared__ float2 smem[];
+    pdl_wait();
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
     const uint64_t row = (uint64_t)blockIdx.x * ROWS + rl;
@@ -84,6 +87,7 @@ k_r2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     TM::sync(rl);
     TM::for_each_out(v, t, [&](int i, float2 x) { sm[spad(i)] = x; });
     TM::sync(rl);
+    pdl_trigger();
     if (!ok) return;
     auto bin = [&](int k, float2 wk) {
         const float2 a = sm[spad(k & (M - 1))];
@@ -130,6 +134,7 @@ k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     constexpr int S = smem_stride<M, E, false>();
     using TM = Team<M, E, true, sync_kind(T, T * ROWS)>;
     extern __shared__ float2 smem[];
+    pdl_wait();
     const int rl = threadIdx.x / T;
     const int t = threadIdx.x - rl * T;
     const uint64_t row = (uint64_t)blockIdx.x * ROWS + rl;
@@ -151,6 +156,7 @@ k_c2r(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     });
     TM::sync(rl);   // the passes reuse the staging buffer for their exchanges
     TM::template passes<0>(v, sm, tw, t, rl);
+    pdl_trigger();
     if (ok) TM::for_each_out(v, t, [&](int i, float2 x) { st_stream(dst + i, x); });
 }
 

@@ -6,6 +6,7 @@
 // (IDFT(x) = conj(DFT(conj x))), so one code path per length serves both directions.
 #include "backend.h"
 #include "fft_kernels.cuh"
+#include "launch.cuh"
 #include "ragged.h"
 #include "tma.cuh"
 
@@ -36,6 +37,7 @@ __device__ __forceinline__ void ragged_tile(const RaggedEntry& r, uint64_t tileI
         const float2 x = ld_stream(src + i);
         return make_float2(x.x, sgn * x.y);
     });
+    pdl_trigger();
     if (ok)
         TM::for_each_out(v, t, [&](int i, float2 x) { st_stream(dst + i, make_float2(x.x * sc, sgn * sc * x.y)); });
 }
@@ -85,6 +87,7 @@ __global__ void __launch_bounds__(kRaggedThreads, 4)
 k_ragged_flat(const RaggedEntry* __restrict__ reqs, int nreq, const uint32_t* __restrict__ tileMap,
               uint64_t tileBase) {
     extern __shared__ float2 smem[];
+    pdl_wait();
     const uint64_t tile = tileBase + blockIdx.x;
     const int q = tileMap ? (int)__ldg(tileMap + tile) : find_request_plain(reqs, nreq, tile);
     const RaggedEntry r = reqs[q];
@@ -164,6 +167,7 @@ __device__ __forceinline__ void ragged_tile_staged(const RaggedEntry& r, uint64_
         issue_tile(reqs, nreq, next, nextStage, bar, slot);
     }
     TM::template passes<0>(v, xbuf + rl * S, static_cast<const float2*>(r.tw), t, rl);
+    pdl_trigger();
     if (ok)
         TM::for_each_out(v, t, [&](int i, float2 x) { st_stream(dst + i, make_float2(x.x * sc, sgn * sc * x.y)); });
 }
@@ -294,8 +298,10 @@ int launchRaggedFlat(const void* entries, int count, const void* tileMap, uint64
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     for (uint64_t base = 0; base < totalTiles; base += 0x7fffffffull) {
         const uint64_t cnt = totalTiles - base < 0x7fffffffull ? totalTiles - base : 0x7fffffffull;
-        dev::k_ragged_flat<<<(unsigned)cnt, kRaggedThreads, raggedSmemBytes(), st>>>(
-            es, count, static_cast<const uint32_t*>(tileMap), base);
+        const uint32_t* map = static_cast<const uint32_t*>(tileMap);
+        if (cudaError_t e = launchPdl((const void*)dev::k_ragged_flat, (unsigned)cnt, kRaggedThreads,
+                                      raggedSmemBytes(), st, es, count, map, base))
+            return (int)e;
     }
     return (int)cudaGetLastError();
 }
