@@ -56,6 +56,11 @@ SIGNATURES = {
     "bfly_plan_exec_istft_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
                                              C.c_uint32, C.c_uint32, C.c_int, C.c_void_p, C.c_uint64,
                                              C.c_float, C.c_void_p]),
+    "bfly_plan_exec_stft_backward_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
+                                                     C.c_uint64, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
+    "bfly_plan_exec_istft_backward_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
+                                                      C.c_uint32, C.c_uint32, C.c_int, C.c_void_p, C.c_uint64,
+                                                      C.c_float, C.c_void_p]),
     "bfly_plan_exec_r2c_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
                                            C.c_float, C.c_float, C.c_void_p]),
     "bfly_plan_exec_c2r_async": (C.c_int, [c_plan, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,

@@ -198,6 +198,21 @@ class Plan:
                                                     1 if center else 0, d_window or None, out_len, scale,
                                                     stream or None)
 
+    def exec_stft_backward(self, d_grad_spec: int, d_grad_sig: int, n: int, signals: int, sig_len: int,
+                           hop: int, center: bool = True, d_window: int = 0, stream: int = 0) -> int:
+        """Gradient of exec_stft's signal from the gradient of its output, one kernel."""
+        return self._lib.bfly_plan_exec_stft_backward_async(self._h, d_grad_spec, d_grad_sig, n, signals, sig_len,
+                                                            hop, 1 if center else 0, d_window or None,
+                                                            stream or None)
+
+    def exec_istft_backward(self, d_grad_out: int, d_grad_spec: int, n: int, signals: int, frames: int, hop: int,
+                            center: bool = True, d_window: int = 0, out_len: int = 0, scale: float = 1.0,
+                            stream: int = 0) -> int:
+        """Gradient of exec_istft's spectrum from the gradient of its output, one kernel."""
+        return self._lib.bfly_plan_exec_istft_backward_async(self._h, d_grad_out, d_grad_spec, n, signals, frames,
+                                                             hop, 1 if center else 0, d_window or None, out_len,
+                                                             scale, stream or None)
+
     def exec_r2c(self, d_in: int, d_out: int, n: int, batch: int, s_edge: float = 1.0,
                  s_int: float = 1.0, stream: int = 0) -> int:
         return self._lib.bfly_plan_exec_r2c_async(self._h, d_in, d_out, n, batch, s_edge, s_int,

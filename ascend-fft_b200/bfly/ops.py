@@ -304,6 +304,10 @@ def ifft(x: torch.Tensor, norm: str | None = None, dim: int = -1) -> torch.Tenso
     return _FFT.apply(x, 1, _scale(norm, x.shape[-1], False))
 
 
+def _pow2(n: int) -> bool:
+    return n >= 64 and n <= 8192 and n & (n - 1) == 0
+
+
 class _STFT(torch.autograd.Function):
     """Framing + window + R2C in one kernel; the window is a constant (no gradient)."""
 
@@ -327,7 +331,18 @@ class _STFT(torch.autograd.Function):
         (window,) = ctx.saved_tensors
         n, hop, length = ctx.n, ctx.hop, ctx.length
         signals, frames = g.shape[0], g.shape[1]
-        # adjoint of each frame's one-sided transform (the weighted C2R of rfft's backward)
+        if _pow2(n) and (length >= n + 2 if ctx.center else length >= n):
+            # one kernel: each frame's weighted C2R, the window, the overlap-add and the fold of
+            # the reflect padding
+            gx = torch.empty(signals, length, dtype=torch.float32, device=g.device)
+            rc = plan_for(g.device, n, "real").exec_stft_backward(
+                g.contiguous().data_ptr(), gx.data_ptr(), n, signals, length, hop, ctx.center,
+                window.data_ptr() if window is not None else 0, _stream(g))
+            if rc:
+                raise BflyError(f"exec_stft_backward(n={n}, signals={signals}, length={length}, hop={hop})", rc)
+            return gx, None, None, None, None
+        # other lengths: the adjoint of each frame's one-sided transform (the weighted C2R of
+        # rfft's backward), then the window, overlap-add and reflect fold
         fr = c2r(g.contiguous().reshape(signals * frames, n // 2 + 1), n, 1.0, 0.5, 1.0)
         fr = fr.reshape(signals, frames, n)
         if window is not None:
@@ -387,6 +402,15 @@ class _ISTFT(torch.autograd.Function):
     def backward(ctx, g):
         (window,) = ctx.saved_tensors
         n, hop, frames = ctx.n, ctx.hop, ctx.frames
+        if _pow2(n):
+            # one kernel: the frames of g / envelope, windowed, transformed and weighted
+            gs = torch.empty(g.shape[0], frames, n // 2 + 1, dtype=torch.complex64, device=g.device)
+            rc = plan_for(g.device, n, "real").exec_istft_backward(
+                g.contiguous().data_ptr(), gs.data_ptr(), n, g.shape[0], frames, hop, ctx.center,
+                window.data_ptr() if window is not None else 0, g.shape[1], ctx.scale, _stream(g))
+            if rc:
+                raise BflyError(f"exec_istft_backward(n={n}, frames={frames}, hop={hop})", rc)
+            return gs, None, None, None, None, None, None
         padded = n + hop * (frames - 1)
         start = n // 2 if ctx.center else 0
         env = _envelope(window, n, hop, frames, g.device)

@@ -218,6 +218,17 @@ void istftSegments(uint32_t n, int rows, uint32_t frames, uint32_t hop, uint64_t
 int launchIstft(const void* spec, void* out, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
                 int64_t start, uint64_t outLen, const void* window, const void* tw, const void* twr, float scale,
                 void* stream);
+// Adjoints for autograd, power-of-two n in [64, 8192], one kernel each.
+// STFT -> signal: gradSpec [signals][frames][n/2+1] -> gradSig [signals][sigLen] (the gradient of
+// launchStft's input; centred needs sigLen >= n + 2).
+int launchStftAdjoint(const void* gradSpec, void* gradSig, uint32_t n, uint64_t signals, uint32_t frames,
+                      uint32_t hop, bool center, uint64_t sigLen, const void* window, const void* tw, const void* twr,
+                      void* stream);
+// inverse STFT -> spectrum: gradOut [signals][outLen] -> gradSpec [signals][frames][n/2+1] (the
+// gradient of launchIstft's input; start and scale as that call's).
+int launchIstftAdjoint(const void* gradOut, void* gradSpec, uint32_t n, uint64_t signals, uint32_t frames,
+                       uint32_t hop, int64_t start, uint64_t outLen, const void* window, const void* tw,
+                       const void* twr, float scale, void* stream);
 
 // Column FFTs: ny-point transforms down the ncols columns of `mats` row-major matrices,
 // element (m, i, col) at m*matStride + i*pitch + col (float2 units).  ny in 32..4096;

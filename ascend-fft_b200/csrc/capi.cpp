@@ -215,6 +215,21 @@ int bfly_plan_exec_istft_async(bfly_plan* plan, const void* d_spec, void* d_out,
     return p.execIstft(d_spec, d_out, n, signals, frames, hop, center != 0, d_window, out_len, scale, stream);
 }
 
+int bfly_plan_exec_stft_backward_async(bfly_plan* plan, const void* d_grad_spec, void* d_grad_sig, uint32_t n,
+                                       uint64_t signals, uint64_t sig_len, uint32_t hop, int center,
+                                       const void* d_window, void* stream) {
+    PLAN_OR_FAIL();
+    return p.execStftBackward(d_grad_spec, d_grad_sig, n, signals, sig_len, hop, center != 0, d_window, stream);
+}
+
+int bfly_plan_exec_istft_backward_async(bfly_plan* plan, const void* d_grad_out, void* d_grad_spec, uint32_t n,
+                                        uint64_t signals, uint32_t frames, uint32_t hop, int center,
+                                        const void* d_window, uint64_t out_len, float scale, void* stream) {
+    PLAN_OR_FAIL();
+    return p.execIstftBackward(d_grad_out, d_grad_spec, n, signals, frames, hop, center != 0, d_window, out_len,
+                               scale, stream);
+}
+
 int bfly_plan_exec_r2c_async(bfly_plan* plan, const void* d_in, void* d_out, uint32_t n,
                              uint64_t batch, float s_edge, float s_int, void* stream) {
     PLAN_OR_FAIL();

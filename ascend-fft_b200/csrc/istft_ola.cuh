@@ -11,6 +11,15 @@
 // end), the rest (N - hop samples) are carried to the next wave in the other half of a
 // ping-pong buffer.  VEC = 4 sums four consecutive samples per thread with float4 shared and
 // global accesses (N, hop, the output length and the frame buffers multiples of 4 / 16 bytes).
+//
+// ADJ: the same sums without the envelope, as the adjoint of an STFT (its gradient with
+// respect to the signal, start = the centring pad).  A centred STFT read reflected samples
+// x[-i] = x[i] and x[L-1+i] = x[L-1-i]: the sums at padded positions before `start` and after
+// the signal fold onto outputs [1, pad] and [L-1-pad, L-2].  Those outputs collect their
+// direct and folded terms in shared fold buffers (shared-memory atomic adds; each gets exactly
+// two terms onto zero, so the sum does not depend on their order) and are stored at the end by
+// the first and the last segment of the signal, which the launch makes span more than N
+// samples so that they own both terms.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -26,6 +35,8 @@ struct IstftSegment {
     const float* window;
     float* dst;
     float *cur, *nxt, *rinv;
+    int pad = 0;                                  // ADJ: fold width (0: no reflect padding)
+    float *foldL = nullptr, *foldR = nullptr;     // ADJ: outputs [0, pad] and [L-1-pad, L-1)
 
     // `scratch`: 2 (N - hop) + hop floats of shared memory (carry pair, then the envelope table).
     __device__ __forceinline__ void init(int n, uint32_t hop_, uint32_t frames_, uint32_t Q, uint32_t segs, int64_t start_,
@@ -46,6 +57,7 @@ struct IstftSegment {
         outLen = outLen_;
         P0 = (int64_t)first * hop;
         end = start + (int64_t)outLen;
+        if (c + 1 == segs) fB = frames;   // a last segment may be longer than Q (ADJ launches)
         P1 = c + 1 == segs ? (padded > end ? padded : end) : (int64_t)fB * hop;
         window = window_;
         dst = out + (uint64_t)s * outLen;
@@ -63,6 +75,52 @@ struct IstftSegment {
             }
             rinv[r] = e > 0.f ? 1.f / e : 0.f;
         }
+    }
+
+    // ADJ set-up: fold buffers of 2 (pad + 1) floats at `scratch`, zeroed (pad = 0: none).
+    __device__ __forceinline__ void initFold(int pad_, float* scratch) {
+        pad = pad_;
+        if (!pad) return;
+        foldL = scratch;
+        foldR = scratch + pad + 1;
+        for (int q = threadIdx.x; q < 2 * (pad + 1); q += CTA) scratch[q] = 0.f;
+    }
+
+    // ADJ: one completed sum at padded position P (this segment's [P0, P1)).
+    __device__ __forceinline__ void emitAdj(int64_t P, float val) {
+        const int64_t L = (int64_t)outLen;
+        int64_t t = P - start;   // output of the direct term
+        if (pad) {
+            if (t < 0) {                       // left padding: the mirror of output -t
+                atomicAdd(foldL - t, val);
+                return;
+            }
+            if (t >= L) {                      // right padding: the mirror of output 2 (L-1) - t
+                atomicAdd(foldR + (2 * (L - 1) - t) - (L - 1 - pad), val);
+                return;
+            }
+            if (t <= pad) {
+                atomicAdd(foldL + t, val);
+                return;
+            }
+            if (t >= L - 1 - pad && t < L - 1) {
+                atomicAdd(foldR + (t - (L - 1 - pad)), val);
+                return;
+            }
+        }
+        if (t >= 0 && t < L) __stcs(dst + t, val);
+    }
+
+    // ADJ: store the fold outputs (after the last wave and zeroTail).
+    __device__ __forceinline__ void finishFold(uint32_t segs) {
+        if (!pad) return;
+        __syncthreads();
+        const int64_t L = (int64_t)outLen;
+        const uint32_t c = blockIdx.x % segs;
+        if (c == 0)
+            for (int u = threadIdx.x; u <= pad; u += CTA) __stcs(dst + u, foldL[u]);
+        if (c + 1 == segs)
+            for (int u = threadIdx.x; u < pad; u += CTA) __stcs(dst + (L - 1 - pad) + u, foldR[u]);
     }
 
     // Samples near either end: the envelope of the frames that exist.
@@ -83,7 +141,7 @@ struct IstftSegment {
     // w[j] x_(f0+r)[j], ld4(r, j) the float4 of samples j .. j+3 (j a multiple of 4).  Called by
     // every thread after a barrier that follows the frames' writes; swaps the carry halves.
     // CTA_C: the block size when known at compile time (0: blockDim.x).
-    template <int VEC, int CTA_C, class Ld1, class Ld4>
+    template <int VEC, int CTA_C, bool ADJ = false, class Ld1, class Ld4>
     __device__ __forceinline__ void wave(uint32_t f0, int R, Ld1&& ld1, Ld4&& ld4) {
         const int cta = CTA_C > 0 ? CTA_C : CTA;
         auto clampq = [](int64_t v, int hi) { return (int)(v < 0 ? 0 : (v > hi ? hi : v)); };
@@ -91,9 +149,10 @@ struct IstftSegment {
         const int span = (R - 1) * (int)hop + N;
         const int done = tail ? span : R * (int)hop;
         const int64_t base = (int64_t)f0 * hop;
-        // span offsets q this CTA stores ([wlo, whi)) and those with the periodic envelope
-        const int wlo = clampq((P0 > start ? P0 : start) - base, done);
-        const int whi = clampq((P1 < end ? P1 : end) - base, done);
+        // span offsets q this CTA stores ([wlo, whi)) and those with the periodic envelope; the
+        // adjoint also emits the padding sums of its segment (folded onto the signal)
+        const int wlo = clampq((ADJ ? P0 : (P0 > start ? P0 : start)) - base, done);
+        const int whi = clampq((ADJ ? P1 : (P1 < end ? P1 : end)) - base, done);
         const int elo = clampq((int64_t)(N - 1) - base, span);
         const int ehi = clampq((int64_t)frames * hop - base, span);
         float* dq = dst + (base - start);   // output of span offset q at dq[q] (wlo <= q < whi)
@@ -113,7 +172,8 @@ struct IstftSegment {
                 if (q >= done) {
                     nxt[q - done] = val;
                 } else if (q >= wlo && q < whi) {
-                    __stcs(dq + q, val * (q >= elo && q < ehi ? rinv[qr] : edgeInv(base + q)));
+                    if constexpr (ADJ) emitAdj(base + q, val);
+                    else __stcs(dq + q, val * (q >= elo && q < ehi ? rinv[qr] : edgeInv(base + q)));
                 }
             } else {
                 float4 val = q < CARRY ? *reinterpret_cast<const float4*>(cur + q) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -129,6 +189,16 @@ struct IstftSegment {
                 }
                 if (q >= done) {
                     *reinterpret_cast<float4*>(nxt + q - done) = val;
+                } else if (ADJ && q >= wlo && q < whi) {
+                    const int64_t t = base + q - start;
+                    if (t >= pad + 1 && t + 3 < (int64_t)outLen - 1 - pad && q + 3 < whi) {
+                        __stcs(reinterpret_cast<float4*>(dq + q), val);
+                    } else {
+                        const float vs[4] = {val.x, val.y, val.z, val.w};
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            if (q + u < whi) emitAdj(base + q + u, vs[u]);
+                    }
                 } else if (q >= wlo && q < whi) {
                     float4 e;
                     if (q >= elo && q + 3 < ehi) {

@@ -833,6 +833,35 @@ int Plan::execStft(const void* dSig, void* dOut, uint32_t n, uint64_t signals, u
     return 0;
 }
 
+int Plan::execStftBackward(const void* dGradSpec, void* dGradSig, uint32_t n, uint64_t signals, uint64_t sigLen,
+                           uint32_t hop, bool center, const void* dWindow, void* stream) {
+    if (!impl_ || !dGradSpec || !dGradSig || signals == 0 || hop == 0 || hop > n || !backend::hasStft(n)) return -8;
+    if (reinterpret_cast<uintptr_t>(dWindow) & 7u) return -8;
+    if (center ? sigLen < (uint64_t)n + 2 : sigLen < n) return -8;
+    const uint64_t frames = center ? 1 + sigLen / hop : 1 + (sigLen - n) / hop;
+    if (frames > 0xFFFFFFFFull || signals * frames > 0xFFFFFFFFull) return -8;
+    if (prepareC2C(n / 2, kColsE) || prepareReal(n)) return -2;
+    if (backend::launchStftAdjoint(dGradSpec, dGradSig, n, signals, (uint32_t)frames, hop, center, sigLen, dWindow,
+                                   impl_->twC2C[{n / 2, kColsE}], impl_->twReal[n], stream))
+        return -5;
+    return 0;
+}
+
+int Plan::execIstftBackward(const void* dGradOut, void* dGradSpec, uint32_t n, uint64_t signals, uint32_t frames,
+                            uint32_t hop, bool center, const void* dWindow, uint64_t outLen, float scale,
+                            void* stream) {
+    if (!impl_ || !dGradOut || !dGradSpec || signals == 0 || frames == 0 || hop == 0 || hop > n ||
+        !backend::hasStft(n))
+        return -8;
+    if (signals * frames > 0xFFFFFFFFull || outLen == 0 || outLen > (1ull << 62)) return -8;
+    if (reinterpret_cast<uintptr_t>(dWindow) & 7u) return -8;
+    if (prepareC2C(n / 2, kColsE) || prepareReal(n)) return -2;
+    if (backend::launchIstftAdjoint(dGradOut, dGradSpec, n, signals, frames, hop, center ? (int64_t)(n / 2) : 0,
+                                    outLen, dWindow, impl_->twC2C[{n / 2, kColsE}], impl_->twReal[n], scale, stream))
+        return -5;
+    return 0;
+}
+
 int Plan::execIstft(const void* dSpec, void* dOut, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
                     bool center, const void* dWindow, uint64_t outLen, float scale, void* stream) {
     const bool mixedN = !pow2(n) && realMixed(n) && n <= backend::kIstftMixedMaxN;

@@ -622,12 +622,20 @@ class Subs:
                                                                  w.data_ptr(), L, 1.0, sh), "istft"))
             ib = S * frames * 8 * (n // 2 + 1) + 4 * S * L
             rt = float((torch.linalg.vector_norm(xb - x) / torch.linalg.vector_norm(x)).item())
-            out[f"n{n}_hop{hop}"] = [round(self.gbs(fb, ms), 1), round(ms, 3), float(f"{e:.3g}"),
-                                     round(self.gbs(ib, ms_i), 1), round(ms_i, 3), float(f"{rt:.3g}")]
+            row = [round(self.gbs(fb, ms), 1), round(ms, 3), float(f"{e:.3g}"),
+                   round(self.gbs(ib, ms_i), 1), round(ms_i, 3), float(f"{rt:.3g}")]
+            if n & (n - 1) == 0:   # the fused gradients (one kernel each)
+                ms_sb = self.timed(lambda: self.check(plan.exec_stft_backward(y.data_ptr(), xb.data_ptr(), n, S, L, hop,
+                                                                             True, w.data_ptr(), sh), "stft_bwd"))
+                ms_ib = self.timed(lambda: self.check(plan.exec_istft_backward(x.data_ptr(), y.data_ptr(), n, S, frames,
+                                                                              hop, True, w.data_ptr(), L, 1.0, sh),
+                                                      "istft_bwd"))
+                row += [round(ms_sb, 3), round(ms_ib, 3)]
+            out[f"n{n}_hop{hop}"] = row
             del x, y, xb
         emit({"sub": "stft", "unit": UNIT, "signals": "4 x 2^24 samples, centred, Hann",
               "cols": ["stft_frame_gbs", "stft_ms", "stft_rel_l2_vs_torch_f64", "istft_gbs", "istft_ms",
-                       "round_trip_rel_l2"], "rows": out})
+                       "round_trip_rel_l2", "stft_backward_ms", "istft_backward_ms"], "rows": out})
 
 
 # ------------------------------------------------------------------ our arm

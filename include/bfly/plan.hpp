@@ -243,6 +243,16 @@ public:
     // last frame, are 0.
     int execIstft(const void* dSpec, void* dOut, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
                   bool center, const void* dWindow, uint64_t outLen, float scale, void* stream);
+    // Gradients for autograd, in one kernel each (n a power of two in [64, 8192]):
+    // execStftBackward: dGradSpec = dL/d(execStft's output) -> dGradSig = dL/d(its signal),
+    // the window multiply, overlap-add and reflect fold of a centred STFT included (centred:
+    // sigLen >= n + 2); execIstftBackward: dGradOut = dL/d(execIstft's output) -> dGradSpec =
+    // dL/d(its spectrum), the envelope division included.  Arguments mean what they mean in
+    // execStft / execIstft; -8 for shapes these kernels do not serve.
+    int execStftBackward(const void* dGradSpec, void* dGradSig, uint32_t n, uint64_t signals, uint64_t sigLen,
+                         uint32_t hop, bool center, const void* dWindow, void* stream);
+    int execIstftBackward(const void* dGradOut, void* dGradSpec, uint32_t n, uint64_t signals, uint32_t frames,
+                          uint32_t hop, bool center, const void* dWindow, uint64_t outLen, float scale, void* stream);
     // R2C [batch][n] -> [batch][n/2+1] complex, bins scaled by (sEdge at 0 and n/2, sInt
     // elsewhere); sEdge = sInt = 1 is the plain transform.  n a power of two in [64, 8192]
     // (single-pass team kernels), or even with n/2 = 2^a 3^b 5^c 7^d 11^e 13^f <= 12288

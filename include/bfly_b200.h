@@ -177,6 +177,22 @@ int bfly_plan_exec_stft_async(bfly_plan* plan, const void* d_sig, void* d_out, u
 int bfly_plan_exec_istft_async(bfly_plan* plan, const void* d_spec, void* d_out, uint32_t n,
                                uint64_t signals, uint32_t frames, uint32_t hop, int center,
                                const void* d_window, uint64_t out_len, float scale, void* stream);
+/* New: gradients of the two calls above for autograd, one kernel each, n a power of two in
+ * [64, 8192] (no counterpart in the reference, which has no STFT or autograd).
+ * stft_backward: d_grad_spec = [signals][frames][n/2+1] complex64, the gradient of a real loss
+ * with respect to exec_stft's output -> d_grad_sig = [signals][sig_len] fp32, the gradient with
+ * respect to its signal (window multiply, overlap-add and, when center != 0, the reflect
+ * padding folded back; then sig_len >= n + 2).
+ * istft_backward: d_grad_out = [signals][out_len] fp32, the gradient with respect to
+ * exec_istft's output -> d_grad_spec = [signals][frames][n/2+1] complex64, the gradient with
+ * respect to its spectrum (envelope division, window, one-sided weights and scale included).
+ * Arguments as in exec_stft / exec_istft; -8 for shapes they do not serve. */
+int bfly_plan_exec_stft_backward_async(bfly_plan* plan, const void* d_grad_spec, void* d_grad_sig, uint32_t n,
+                                       uint64_t signals, uint64_t sig_len, uint32_t hop, int center,
+                                       const void* d_window, void* stream);
+int bfly_plan_exec_istft_backward_async(bfly_plan* plan, const void* d_grad_out, void* d_grad_spec, uint32_t n,
+                                        uint64_t signals, uint32_t frames, uint32_t hop, int center,
+                                        const void* d_window, uint64_t out_len, float scale, void* stream);
 /* R2C [batch][n] -> [batch][n/2+1] complex, n a power of two in [64, 8192], or even with n/2
  * = 2^a 3^b 5^c 7^d 11^e 13^f up to 12288 (mixed-radix passes; the reference supports powers of
  * two only); bins 0 and n/2 scaled by s_edge, the others by s_int (1, 1 for the plain transform). */

@@ -321,6 +321,61 @@ int launchIstft(const void* spec, void* out, uint32_t n, uint64_t signals, uint3
     istftDirect(spec, out, n, signals, frames, hop, start, outLen, window, scale);
     return 0;
 }
+// Adjoints by their definitions (direct sums; the device kernels are checked against torch).
+int launchStftAdjoint(const void* gradSpec, void* gradSig, uint32_t n, uint64_t signals, uint32_t frames,
+                      uint32_t hop, bool center, uint64_t sigLen, const void* window, const void*, const void*,
+                      void*) {
+    if (!hasStft(n) || hop == 0 || hop > n || frames == 0 || (center && sigLen < (uint64_t)n + 2)) return 1;
+    if (int r = launch()) return r;
+    const float* w = (const float*)window;
+    std::vector<float> fr((size_t)frames * n);
+    for (uint64_t s = 0; s < signals; ++s) {
+        c2rDirect((const float*)gradSpec + s * frames * (n + 2), fr.data(), n, frames, 1.f, 0.5f, 1.f);
+        float* g = (float*)gradSig + s * sigLen;
+        for (uint64_t i = 0; i < sigLen; ++i) g[i] = 0.f;
+        for (uint32_t f = 0; f < frames; ++f)
+            for (uint32_t j = 0; j < n; ++j) {
+                long long i = (long long)f * hop + j - (center ? n / 2 : 0);
+                if (i < 0) i = -i;
+                if (i >= (long long)sigLen) i = 2 * ((long long)sigLen - 1) - i;
+                g[i] += (w ? w[j] : 1.f) * fr[(size_t)f * n + j];
+            }
+    }
+    return 0;
+}
+int launchIstftAdjoint(const void* gradOut, void* gradSpec, uint32_t n, uint64_t signals, uint32_t frames,
+                       uint32_t hop, int64_t start, uint64_t outLen, const void* window, const void*, const void*,
+                       float scale, void*) {
+    if (!hasStft(n) || hop == 0 || hop > n || frames == 0) return 1;
+    if (int r = launch()) return r;
+    const float* w = (const float*)window;
+    const float c = scale / (float)n;
+    std::vector<float> frame(2 * n), spec(2 * n);
+    for (uint64_t s = 0; s < signals; ++s)
+        for (uint32_t f = 0; f < frames; ++f) {
+            for (uint32_t j = 0; j < n; ++j) {
+                const long long p = (long long)f * hop + j, i = p - start;
+                double env = 0;
+                for (uint32_t g = 0; g < frames; ++g) {
+                    const long long jj = p - (long long)g * hop;
+                    if (jj >= 0 && jj < (long long)n) env += (w ? w[jj] : 1.0) * (w ? w[jj] : 1.0);
+                }
+                const float h = (i >= 0 && i < (long long)outLen && env > 0)
+                                    ? (float)(((const float*)gradOut)[s * outLen + i] / env) : 0.f;
+                frame[2 * j] = h * (w ? w[j] : 1.f);
+                frame[2 * j + 1] = 0.f;
+            }
+            dft(frame.data(), spec.data(), n, -1, 1.f);
+            float* o = (float*)gradSpec + 2 * ((s * frames + f) * (n / 2 + 1));
+            for (uint32_t k = 0; k <= n / 2; ++k) {
+                const float wt = (k == 0 || k == n / 2) ? c : 2.f * c;
+                o[2 * k] = spec[2 * k] * wt;
+                o[2 * k + 1] = spec[2 * k + 1] * wt;
+            }
+        }
+    return 0;
+}
+
 static void istftDirect(const void* spec, void* out, uint32_t n, uint64_t signals, uint32_t frames, uint32_t hop,
                         int64_t start, uint64_t outLen, const void* window, float scale) {
     const float* w = (const float*)window;
