@@ -217,9 +217,10 @@ int bfly_plan_exec_c2c_tc_async(bfly_plan* plan, const void* d_in, void* d_out, 
 /* Status word of the tensor-core launches on the current device: 0, or 1 when a bounded wait
  * for an MMA ran out (the launch then stopped early); reading clears it. */
 int bfly_tc_device_status(unsigned* status);
-/* Status word of the single-pass long C2C (one thread-block cluster per row, n 8192..65536)
- * on the current device: 0, or 1 when a bounded wait of the kernel ran out (that launch's
- * output is invalid); reading clears it.  The reference has no counterpart (its long path,
+/* Status word of the single-launch long C2C schedules on the current device: 0, bit 1 when a
+ * bounded wait of the cluster kernel (one thread-block cluster per row) ran out, bit 2 when one
+ * of the ring kernel (both four-step passes in one launch) did (that launch's output is
+ * invalid); reading clears it.  The reference has no counterpart (its long path,
  * src/host/fft_check.cpp:843-970, is a sequence of global-memory passes). */
 int bfly_long_device_status(unsigned* status);
 
