@@ -415,8 +415,14 @@ class Subs:
                     ms = self.timed(fn)
                     res.append((ms, self.gbs(byts, ms), self.err(y, x)))
                 (ms0, g0, e0), (_, g3, e3), (_, g2, e2) = res
+                # the autotuner's plan for this (n, batch): candidates measured, FP64-checked, best kept
+                tuned = self.ctx.select(n, b, 8)
+                ms_t = self.timed(lambda: self.check(tuned.exec_c2c(x.data_ptr(), y.data_ptr(), n, b, -1, 1.0, sh), "tuned"))
+                et = self.err(y, x)
+                tuned.close()
                 rows.append([n, b, round(ms0 * 1e3, 2), round(g0, 1), round(g0 / peak, 3), float(f"{e0:.3g}"),
-                             round(g3, 1), float(f"{e3:.3g}"), round(g2, 1), float(f"{e2:.3g}")])
+                             round(g3, 1), float(f"{e3:.3g}"), round(g2, 1), float(f"{e2:.3g}"),
+                             round(ms_t * 1e3, 2), float(f"{et:.3g}")])
                 sp = g3 / g0
                 if best is None or sp > best[0]:
                     best = (sp, n, b, e3)
@@ -424,13 +430,15 @@ class Subs:
         meets = sum(1 for r in rows if r[4] >= 0.70)
         emit({"sub": "c2c_grid49_points", "unit": UNIT, "peak": peak,
               "cols": ["n", "b", "fp32_us", "fp32_gbs", "fp32_frac", "fp32_rel_l2", "tc3_gbs", "tc3_rel_l2",
-                       "tc2_gbs", "tc2_rel_l2"], "rows": rows, "fp32_points_at_0.70": meets,
+                       "tc2_gbs", "tc2_rel_l2", "tuned_us", "tuned_rel_l2"], "rows": rows, "fp32_points_at_0.70": meets,
+              "tuned": "Context.select(n, batch): the autotuner's plan for the point (fp32 columns: the per-length plan)",
               "l2": "points under 126 MB are L2-warm across the 20 back-to-back launches of the graph"})
         b4096 = [r for r in rows if r[1] == 4096]
         self.summary["grid49_points"] = {
             "fp32_frac_at_b4096": [r[4] for r in b4096], "fp32_points_at_0.70": meets,
             "tc3_vs_fp32_at_b4096": [round(r[6] / r[3], 2) for r in b4096],
             "tc3_best_speedup": [round(best[0], 3), best[1], best[2]],
+            "tuned_vs_per_length_time": round(sum(r[10] for r in rows) / sum(r[2] for r in rows), 3),
             "tc3_max_rel_l2": max(r[7] for r in rows), "tc2_max_rel_l2": max(r[9] for r in rows)}
 
     # -- config 4: the 256-request mix in one launch, against one launch per request

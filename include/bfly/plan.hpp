@@ -39,7 +39,7 @@ struct Hardware {
 // ---------------------------------------------------------------- A: mapping
 struct Mapping {
     int ctaThreads = 256;                  // threads per CTA
-    std::string localExchange = "shared";  // shared | shuffle (not lowered)
+    std::string localExchange = "shared";  // shared (the only lowering)
     int level = 0;                         // 0 = one GPU (batch sharding lives above the plan)
     bool validate(const Hardware& hw, std::string* why) const;
 };

@@ -89,10 +89,15 @@ int streamSync(void*) {
     return fake::syncs == fake::failSync ? 1 : 0;
 }
 
-struct Timer { int dummy; };
+// Elapsed time: timerMs per kernel launched between start and stop (at least one).
+struct Timer { int launchesAtStart; };
 int timerCreate(Timer** t) { *t = new Timer{0}; return 0; }
-int timerStart(Timer*, void*) { return 0; }
-int timerStop(Timer*, void*, float* ms) { *ms = fake::timerMs; return 0; }
+int timerStart(Timer* t, void*) { t->launchesAtStart = fake::launches; return 0; }
+int timerStop(Timer* t, void*, float* ms) {
+    const int k = fake::launches - t->launchesAtStart;
+    *ms = fake::timerMs * (float)(k > 1 ? k : 1);
+    return 0;
+}
 void timerDestroy(Timer* t) { delete t; }
 
 bool hasVariant(int kind, uint32_t n, int e, int cta) {
