@@ -135,7 +135,7 @@ class ClockSampler:
 
     def __init__(self, index: int, bus_id: str | None = None):
         self.index, self.bus_id = index, bus_id
-        self.samples, self.times, self.reasons, self.max_mhz = [], [], set(), None
+        self.samples, self.times, self.masks, self.reasons, self.max_mhz = [], [], [], set(), None
         self.window = None   # (t0, t1) host time of the timed region
         self._stop = threading.Event()
         self._thread = None
@@ -146,14 +146,12 @@ class ClockSampler:
             try:
                 t = time.perf_counter()
                 self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
-                self.times.append(t)
                 mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                for bit, name in self.REASONS.items():
-                    if mask & bit:
-                        self.reasons.add(name)
+                self.times.append(0.5 * (t + time.perf_counter()))
+                self.masks.append(mask)
             except Exception:
                 pass
-            time.sleep(0.0002)
+            time.sleep(0.0001)
 
     def __enter__(self):
         try:
@@ -216,11 +214,16 @@ class ClockSampler:
         warm-up's samples stand in when none did."""
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
-        inside = self.samples
+        inside = list(range(len(self.samples)))
         if self.window:
-            inside = [c for c, t in zip(self.samples, self.times) if self.window[0] <= t <= self.window[1]]
-        return {"sm_mhz": statistics.median(inside or self.samples), "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(self.reasons), "samples": len(self.samples),
+            inside = [i for i, t in enumerate(self.times) if self.window[0] <= t <= self.window[1]]
+        use = inside or list(range(len(self.samples)))
+        reasons = set(self.reasons)
+        for i in use:
+            if i < len(self.masks):
+                reasons |= {name for bit, name in self.REASONS.items() if self.masks[i] & bit}
+        return {"sm_mhz": statistics.median(self.samples[i] for i in use), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(self.samples),
                 "samples_in_timed_region": len(inside) if self.window else len(self.samples)}
 
 
@@ -555,9 +558,15 @@ class Subs:
             ms_r = self.timed(lambda: self.check(ring.exec_c2c(x.data_ptr(), z.data_ptr(), n, b, -1, 1.0, sh), "ring"))
             res[n] += [round(self.gbs(byts, ms_r), 1), float(f"{self.err(z, x, rows=2):.3g}")]
             ring.close()
+            # context: the GPU's library FFT (cuFFT through torch.fft) forward and inverse, same tensors
+            with torch.cuda.stream(self.stream):
+                ms_cf = self.timed(lambda: torch.fft.fft(x, out=y))
+                ms_cb = self.timed(lambda: torch.fft.ifft(y, out=z))
+            res[n] += [round(self.gbs(byts, ms_cf), 1), round(self.gbs(byts, ms_cb), 1)]
             del x, y, z
         emit({"sub": "long_fwd_bwd", "unit": UNIT,
-              "cols": ["fwd_gbs", "bwd_gbs", "fwd_rel_l2", "bwd_rel_l2", "ring_fwd_gbs", "ring_rel_l2"],
+              "cols": ["fwd_gbs", "bwd_gbs", "fwd_rel_l2", "bwd_rel_l2", "ring_fwd_gbs", "ring_rel_l2",
+                       "cufft_fwd_gbs", "cufft_inv_gbs"],
               "schedule": "single pass n <= 16384, two-kernel four-step above; ring = one-launch four-step",
               "rows": {f"n{n}_b{(1 << 26) // n}": v for n, v in res.items()}})
         self.summary["long_fwd_bwd_frac"] = {str(n): [round(v[0] / peak, 3), round(v[1] / peak, 3)] for n, v in res.items()}
@@ -661,6 +670,10 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     import bfly
 
+    # clock sampling runs from here to the end of the headline's timed region (which lasts a
+    # few ms): the sampler is warm when the region starts, and only its samples inside count
+    bus = getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None)
+    clock_sampler = ClockSampler(dev.index, bus).__enter__()
     ctx = bfly.Context()
     rc = ctx.init(device=dev.index)
     if rc:
@@ -718,10 +731,7 @@ def run_ours(args):
     worst = max(worst, check("ragged"))
 
     def timed(fn, steps, sample_clocks=False):
-        bus = getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None)
-        sampler = ClockSampler(dev.index, bus) if sample_clocks else None
-        if sampler:   # sampling from before the warm-up: the timed region itself lasts a few ms
-            sampler.__enter__()
+        sampler = clock_sampler if sample_clocks else None
         for _ in range(max(3, args.warmup)):
             fn()
         stream.synchronize()
@@ -882,6 +892,7 @@ def run_ours(args):
                      "traffic": (tr + tw) if tr is not None else None, "traffic_read": tr,
                      "traffic_note": "ncu dram bytes inside the launch; writes left dirty in L2 drain after it",
                      "kernel": "k_ragged_flat", "peak_kind": peak_kind, "algorithmic_bytes": grid_bytes()},
+        "gsamples_per_s": round(sum(n * b for n in GRID_N for b in GRID_B) * world / (ms / 1e3) / 1e9, 1),
         "per_point_graph": {"value": round(per_point_gbs, 1), "launches_per_step": len(pts)},
         "largest_launch": {"kernel": "k_c2c N=4096 batch=4096",
                            "frac": round(dom_bytes / (dom_ms / 1e3) / 1e9 / peak, 4),

@@ -34,3 +34,20 @@ def test_reference_arm_other_ranks_are_silent():
     r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_clock_summary_uses_the_timed_window():
+    """Clock samples outside the timed window do not count toward the median or the reasons."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    c = bench.ClockSampler(0)
+    c.samples = [1000, 1965, 1965, 1400]
+    c.times = [0.0, 1.0, 1.5, 3.0]
+    c.masks = [0x4, 0, 0, 0x40]          # sw_power_cap before, hw_thermal_slowdown after the window
+    c.max_mhz = 1965
+    c.window = (0.9, 2.0)
+    s = c.summary()
+    assert s["sm_mhz"] == 1965 and s["reasons"] == [] and s["samples_in_timed_region"] == 2
+    c.window = (5.0, 6.0)                # no sample inside: every sample stands in
+    s = c.summary()
+    assert s["samples_in_timed_region"] == 0 and "hw_thermal_slowdown" in s["reasons"]
