@@ -840,7 +840,7 @@ int Plan::execStftBackward(const void* dGradSpec, void* dGradSig, uint32_t n, ui
     if (reinterpret_cast<uintptr_t>(dWindow) & 7u) return -8;
     if (center ? sigLen < (uint64_t)n + 2 : sigLen < n) return -8;
     const uint64_t frames = center ? 1 + sigLen / hop : 1 + (sigLen - n) / hop;
-    if (frames > 0xFFFFFFFFull || signals * frames > 0xFFFFFFFFull) return -8;
+    if (frames > 0xFFFFFFFFull || signals > 0xFFFFFFFFull / frames) return -8;
     if (prepareC2C(n / 2, kColsE) || prepareReal(n)) return -2;
     if (backend::launchStftAdjoint(dGradSpec, dGradSig, n, signals, (uint32_t)frames, hop, center, sigLen, dWindow,
                                    impl_->twC2C[{n / 2, kColsE}], impl_->twReal[n], stream))
@@ -854,7 +854,7 @@ int Plan::execIstftBackward(const void* dGradOut, void* dGradSpec, uint32_t n, u
     if (!impl_ || !dGradOut || !dGradSpec || signals == 0 || frames == 0 || hop == 0 || hop > n ||
         !backend::hasStft(n))
         return -8;
-    if (signals * frames > 0xFFFFFFFFull || outLen == 0 || outLen > (1ull << 62)) return -8;
+    if (signals > 0xFFFFFFFFull / frames || outLen == 0 || outLen > (1ull << 62)) return -8;
     if (reinterpret_cast<uintptr_t>(dWindow) & 7u) return -8;
     if (prepareC2C(n / 2, kColsE) || prepareReal(n)) return -2;
     if (backend::launchIstftAdjoint(dGradOut, dGradSpec, n, signals, frames, hop, center ? (int64_t)(n / 2) : 0,
@@ -869,7 +869,7 @@ int Plan::execIstft(const void* dSpec, void* dOut, uint32_t n, uint64_t signals,
     if (!impl_ || !dSpec || !dOut || signals == 0 || frames == 0 || hop == 0 || hop > n ||
         !(backend::hasStft(n) || mixedN))
         return -8;
-    if (signals * frames > 0xFFFFFFFFull || outLen == 0 || outLen > (1ull << 62)) return -8;
+    if (signals > 0xFFFFFFFFull / frames || outLen == 0 || outLen > (1ull << 62)) return -8;
     if (reinterpret_cast<uintptr_t>(dWindow) & 7u) return -8;   // the kernels read the window as float2
     if (mixedN) {
         if (prepareMixed(n / 2) || prepareReal(n)) return -2;

@@ -597,6 +597,11 @@ int main(int argc, char** argv) {
         CHECK(plan->execIstft(d, d, 34, 1, frames, hop, true, nullptr, len, 1.f, nullptr) == -8);   // 17 is not 13-smooth
         CHECK(plan->execIstft(d, d, n, 1, frames, 0, true, nullptr, len, 1.f, nullptr) == -8);     // hop 0
         CHECK(plan->execIstft(d, d, n, 1, frames, n + 1, true, nullptr, len, 1.f, nullptr) == -8); // hop above n
+        // signals * frames wraps to a small value in 64 bits: still too many rows
+        CHECK(plan->execIstft(d, d, n, (1ull << 63) + 1, 2, hop, true, nullptr, len, 1.f, nullptr) == -8);
+        CHECK(plan->execIstftBackward(d, d, n, (1ull << 63) + 1, 2, hop, true, nullptr, len, 1.f, nullptr) == -8);
+        CHECK(plan->execStftBackward(d, d, n, (1ull << 62) + 1, 4 * (uint64_t)hop, hop, false, nullptr, nullptr) == -8);
+        CHECK(plan->execStftBackward(d, d, n, 1, n + 1, hop, true, nullptr, nullptr) == -8);   // centred: n + 2 samples
         CHECK(plan->execIstft(d, d, n, 0, frames, hop, true, nullptr, len, 1.f, nullptr) == -8);   // no signals
         CHECK(plan->execIstft(d, d, n, 1, 0, hop, true, nullptr, len, 1.f, nullptr) == -8);        // no frames
         CHECK(plan->execIstft(d, d, n, 1, frames, hop, true, nullptr, 0, 1.f, nullptr) == -8);     // empty output
