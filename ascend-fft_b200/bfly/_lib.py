@@ -75,6 +75,11 @@ SIGNATURES = {
                                    C.POINTER(C.c_int)]),
     "bfly_ragged_device_status": (C.c_int, [C.POINTER(C.c_uint)]),
     "bfly_ragged_destroy": (None, [C.c_void_p]),
+    "bfly_ragged_create_config": (C.c_int, [c_plan, C.c_void_p, C.c_size_t, C.c_int, C.c_uint32,
+                                            C.POINTER(C.c_void_p)]),
+    "bfly_context_tune_ragged": (C.c_int, [C.c_void_p, c_plan, C.c_void_p, C.c_size_t,
+                                           C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "bfly_ragged_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint32)]),
     "bfly_exec_c2c_long_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64,
                                              C.c_int, C.c_float, C.c_void_p]),
     "bfly_max_rel_scaled": (C.c_double, [C.c_void_p, C.c_void_p, C.c_size_t]),

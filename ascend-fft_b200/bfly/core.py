@@ -83,6 +83,20 @@ class Context:
         rc = self._lib.bfly_context_make_plan(self._h, n, batch, candidate_id.encode(), C.byref(p))
         return Plan(self, p) if rc == 0 else None
 
+    def tune_ragged(self, plan, requests, want_log: bool = False):
+        """Autotuned ragged work list over `requests` (as Plan.make_ragged) on `plan`: the
+        launch mode and per-length radices measured fastest on these requests
+        (bfly_context_tune_ragged).  Runs the list many times; outputs are overwritten."""
+        arr = _ragged_array(requests)
+        h = C.c_void_p()
+        log = C.create_string_buffer(1 << 14) if want_log else None
+        rc = self._lib.bfly_context_tune_ragged(self._h, plan._h, arr, len(arr), C.byref(h), log,
+                                                len(log) if log is not None else 0)
+        if rc:
+            raise BflyError("bfly_context_tune_ragged", rc)
+        rg = Ragged(plan, h)
+        return (rg, log.value.decode()) if want_log else rg
+
     def set_tuning_cache(self, path) -> None:
         self._lib.bfly_context_set_tuning_cache(self._h, str(path).encode() if path else b"")
 
@@ -246,17 +260,22 @@ class Plan:
             raise BflyError("bfly_long_device_status", rc)
         return st.value
 
-    def make_ragged(self, requests):
+    def make_ragged(self, requests, mode=None, radix8=None):
         """requests: iterable of (d_in, d_out, n, batch, direction, scale) with device
-        pointers; returns a Ragged whose exec(stream) is one persistent kernel launch."""
-        reqs = list(requests)
-        arr = (_lib.RaggedRequest * len(reqs))()
-        for i, (din, dout, n, b, d, sc) in enumerate(reqs):
-            arr[i] = _lib.RaggedRequest(din, dout, n, d, b, sc, 0)
+        pointers; returns a Ragged whose exec(stream) is one persistent kernel launch.
+        mode / radix8 give an explicit launch configuration (bfly_ragged_create_config);
+        left out, the default applies."""
+        arr = _ragged_array(requests)
         h = C.c_void_p()
-        rc = self._lib.bfly_ragged_create(self._h, arr, len(reqs), C.byref(h))
+        if mode is None and radix8 is None:
+            rc = self._lib.bfly_ragged_create(self._h, arr, len(arr), C.byref(h))
+            what = "bfly_ragged_create"
+        else:
+            rc = self._lib.bfly_ragged_create_config(self._h, arr, len(arr), -1 if mode is None else mode,
+                                                     0x3 if radix8 is None else radix8, C.byref(h))
+            what = "bfly_ragged_create_config"
         if rc:
-            raise BflyError("bfly_ragged_create", rc)
+            raise BflyError(what, rc)
         return Ragged(self, h)
 
     def close(self):
@@ -269,6 +288,14 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def _ragged_array(requests):
+    reqs = list(requests)
+    arr = (_lib.RaggedRequest * len(reqs))()
+    for i, (din, dout, n, b, d, sc) in enumerate(reqs):
+        arr[i] = _lib.RaggedRequest(din, dout, n, d, b, sc, 0)
+    return arr
 
 
 class Ragged:
@@ -287,7 +314,9 @@ class Ragged:
         grid = C.c_int()
         stages = C.c_int()
         self._lib.bfly_ragged_info(self._h, C.byref(tiles), C.byref(grid), C.byref(stages))
-        return {"tiles": tiles.value, "grid": grid.value, "stages": stages.value}
+        radix8 = C.c_uint32()
+        self._lib.bfly_ragged_config(self._h, None, C.byref(radix8))
+        return {"tiles": tiles.value, "grid": grid.value, "stages": stages.value, "radix8": radix8.value}
 
     def device_status(self) -> int:
         """0, or 1 when a staged launch gave up on a bounded wait (reading clears it)."""

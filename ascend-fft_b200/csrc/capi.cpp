@@ -253,18 +253,62 @@ int bfly_plan_exec_c2c_tc_async(bfly_plan* plan, const void* d_in, void* d_out, 
 int bfly_tc_device_status(unsigned* status) { return bfly::Plan::tensorStatus(status); }
 int bfly_long_device_status(unsigned* status) { return bfly::Plan::longStatus(status); }
 
+static std::vector<bfly::RaggedRequest> raggedRequests(const bfly_ragged_request* reqs, size_t count) {
+    std::vector<bfly::RaggedRequest> rs(count);
+    for (size_t i = 0; i < count; ++i)
+        rs[i] = {reqs[i].d_in, reqs[i].d_out, reqs[i].n, reqs[i].batch, reqs[i].direction, reqs[i].scale};
+    return rs;
+}
+
 int bfly_ragged_create(bfly_plan* plan, const bfly_ragged_request* reqs, size_t count,
                        bfly_ragged** out) {
     if (!plan || !plan->plan || !out) return -10;
     *out = nullptr;
     if (!reqs || count == 0) return -8;
-    std::vector<bfly::RaggedRequest> rs(count);
-    for (size_t i = 0; i < count; ++i)
-        rs[i] = {reqs[i].d_in, reqs[i].d_out, reqs[i].n, reqs[i].batch, reqs[i].direction, reqs[i].scale};
+    const auto rs = raggedRequests(reqs, count);
     int status = 0;
     auto r = plan->plan->makeRagged(rs.data(), count, &status);
     if (!r) return status ? status : -1;
     *out = new bfly_ragged{std::move(r)};
+    return 0;
+}
+
+int bfly_ragged_create_config(bfly_plan* plan, const bfly_ragged_request* reqs, size_t count, int mode,
+                              uint32_t radix8, bfly_ragged** out) {
+    if (!plan || !plan->plan || !out) return -10;
+    *out = nullptr;
+    if (!reqs || count == 0) return -8;
+    const auto rs = raggedRequests(reqs, count);
+    bfly::RaggedConfig cfg;
+    cfg.mode = mode;
+    cfg.radix8 = radix8;
+    int status = 0;
+    auto r = plan->plan->makeRagged(rs.data(), count, &status, &cfg);
+    if (!r) return status ? status : -1;
+    *out = new bfly_ragged{std::move(r)};
+    return 0;
+}
+
+int bfly_context_tune_ragged(bfly_context* ctx, bfly_plan* plan, const bfly_ragged_request* reqs, size_t count,
+                             bfly_ragged** out, char* log, size_t log_cap) {
+    if (!ctx || !plan || !plan->plan || !out) return -10;
+    *out = nullptr;
+    if (!reqs || count == 0) return -8;
+    const auto rs = raggedRequests(reqs, count);
+    std::string text;
+    int status = 0;
+    auto r = ctx->ctx.tuneRagged(*plan->plan, rs.data(), count, &status, log ? &text : nullptr);
+    if (log) copyOut(text, log, log_cap, nullptr);
+    if (!r) return status ? status : -1;
+    *out = new bfly_ragged{std::move(r)};
+    return 0;
+}
+
+int bfly_ragged_config(bfly_ragged* ragged, int* mode, uint32_t* radix8) {
+    if (!ragged || !ragged->ragged) return -10;
+    const bfly::RaggedConfig c = ragged->ragged->config();
+    if (mode) *mode = c.mode;
+    if (radix8) *radix8 = c.radix8;
     return 0;
 }
 

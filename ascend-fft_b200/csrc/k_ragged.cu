@@ -1,7 +1,8 @@
 // Ragged persistent launch: a work list of C2C requests with different lengths (32..4096),
 // batch counts and directions, processed by one grid of persistent CTAs.  Every tile is
-// 256 threads x E values (rows of one request; E = raggedE(log2 n)), so tiles cost about the
-// same and a static stride over the tile space balances the grid; no atomics and no waits.
+// 256 threads x E values (rows of one request; E = 8 or 16, chosen per request in the work
+// list), so tiles cost about the same and a static stride over the tile space balances the
+// grid; no atomics and no waits.
 // Inverse requests run the forward kernel on conj(x) and conjugate the result
 // (IDFT(x) = conj(DFT(conj x))), so one code path per length serves both directions.
 #include "backend.h"
@@ -16,9 +17,22 @@ namespace dev {
 // Nonzero after a staged launch gave up on a bounded wait (read and cleared by the host).
 __device__ unsigned int g_ragged_status;
 
-template <int N>
+// Every (length, radix) variant of the work list, as case labels of a switch on
+// logn * 32 + e; CALL(N, E) is the body for one variant.
+#define BFLY_RAGGED_CASES(CALL)                                                              \
+    case 5 * 32 + 8: CALL(32, 8); break;      case 5 * 32 + 16: CALL(32, 16); break;         \
+    case 6 * 32 + 8: CALL(64, 8); break;      case 6 * 32 + 16: CALL(64, 16); break;         \
+    case 7 * 32 + 8: CALL(128, 8); break;     case 7 * 32 + 16: CALL(128, 16); break;        \
+    case 8 * 32 + 8: CALL(256, 8); break;     case 8 * 32 + 16: CALL(256, 16); break;        \
+    case 9 * 32 + 8: CALL(512, 8); break;     case 9 * 32 + 16: CALL(512, 16); break;        \
+    case 10 * 32 + 8: CALL(1024, 8); break;   case 10 * 32 + 16: CALL(1024, 16); break;      \
+    case 11 * 32 + 8: CALL(2048, 8); break;   case 11 * 32 + 16: CALL(2048, 16); break;      \
+    case 12 * 32 + 16: CALL(4096, 16); break;                                                \
+    default: break;
+
+template <int N, int E>
 __device__ __forceinline__ void ragged_tile(const RaggedEntry& r, uint64_t tileInReq, float2* smem) {
-    constexpr int E = raggedE(ilog2c(N));
+    static_assert(raggedVariant(ilog2c(N), E), "no such ragged variant");
     constexpr int T = N / E;
     constexpr int ROWS = kRaggedThreads / T;
     constexpr int S = smem_stride<N, E, false>();
@@ -64,17 +78,9 @@ k_ragged(const RaggedEntry* __restrict__ reqs, int nreq, uint64_t totalTiles) {
         }
         const RaggedEntry r = reqs[lo];
         const uint64_t local = tile - r.tile0;
-        switch (r.logn) {
-            case 5: ragged_tile<32>(r, local, smem); break;
-            case 6: ragged_tile<64>(r, local, smem); break;
-            case 7: ragged_tile<128>(r, local, smem); break;
-            case 8: ragged_tile<256>(r, local, smem); break;
-            case 9: ragged_tile<512>(r, local, smem); break;
-            case 10: ragged_tile<1024>(r, local, smem); break;
-            case 11: ragged_tile<2048>(r, local, smem); break;
-            case 12: ragged_tile<4096>(r, local, smem); break;
-            default: break;
-        }
+#define BFLY_TILE(NN, EE) ragged_tile<NN, EE>(r, local, smem)
+        switch (r.logn * 32 + r.e) { BFLY_RAGGED_CASES(BFLY_TILE) }
+#undef BFLY_TILE
         __syncthreads();   // the next tile reuses the exchange buffers
     }
 }
@@ -92,17 +98,9 @@ k_ragged_flat(const RaggedEntry* __restrict__ reqs, int nreq, const uint32_t* __
     const int q = tileMap ? (int)__ldg(tileMap + tile) : find_request_plain(reqs, nreq, tile);
     const RaggedEntry r = reqs[q];
     const uint64_t local = tile - r.tile0;
-    switch (r.logn) {
-        case 5: ragged_tile<32>(r, local, smem); break;
-        case 6: ragged_tile<64>(r, local, smem); break;
-        case 7: ragged_tile<128>(r, local, smem); break;
-        case 8: ragged_tile<256>(r, local, smem); break;
-        case 9: ragged_tile<512>(r, local, smem); break;
-        case 10: ragged_tile<1024>(r, local, smem); break;
-        case 11: ragged_tile<2048>(r, local, smem); break;
-        case 12: ragged_tile<4096>(r, local, smem); break;
-        default: break;
-    }
+#define BFLY_TILE(NN, EE) ragged_tile<NN, EE>(r, local, smem)
+    switch (r.logn * 32 + r.e) { BFLY_RAGGED_CASES(BFLY_TILE) }
+#undef BFLY_TILE
 }
 
 // ------------------------------------------------------------------ TMA-staged variant
@@ -138,12 +136,11 @@ __device__ __forceinline__ void issue_tile(const RaggedEntry* __restrict__ reqs,
     bulk_load(stage, static_cast<const float2*>(r.in) + first * n, bytes, bar);
 }
 
-template <int N>
+template <int N, int E>
 __device__ __forceinline__ void ragged_tile_staged(const RaggedEntry& r, uint64_t tileInReq, const float2* stage,
                                                    float2* xbuf, const RaggedEntry* __restrict__ reqs, int nreq,
                                                    uint64_t next, uint64_t totalTiles, float2* nextStage,
                                                    uint64_t* bar, int* slot) {
-    constexpr int E = raggedE(ilog2c(N));
     constexpr int T = N / E;
     constexpr int ROWS = kRaggedThreads / T;
     constexpr int S = smem_stride<N, E, false>();
@@ -215,18 +212,9 @@ k_ragged_tma(const RaggedEntry* __restrict__ reqs, int nreq, uint64_t totalTiles
         const uint64_t local = tile - r.tile0;
         const uint64_t next = tile + (uint64_t)STAGES * grid;
         if (threadIdx.x == 0 && next < totalTiles) ++issued[s];
-#define BFLY_STAGED(NN) ragged_tile_staged<NN>(r, local, stage(s), xbuf, reqs, nreq, next, totalTiles, stage(s), &bar[s], &slot[s])
-        switch (r.logn) {
-            case 5: BFLY_STAGED(32); break;
-            case 6: BFLY_STAGED(64); break;
-            case 7: BFLY_STAGED(128); break;
-            case 8: BFLY_STAGED(256); break;
-            case 9: BFLY_STAGED(512); break;
-            case 10: BFLY_STAGED(1024); break;
-            case 11: BFLY_STAGED(2048); break;
-            case 12: BFLY_STAGED(4096); break;
-            default: break;
-        }
+#define BFLY_STAGED(NN, EE) \
+    ragged_tile_staged<NN, EE>(r, local, stage(s), xbuf, reqs, nreq, next, totalTiles, stage(s), &bar[s], &slot[s])
+        switch (r.logn * 32 + r.e) { BFLY_RAGGED_CASES(BFLY_STAGED) }
 #undef BFLY_STAGED
         __syncthreads();   // the next tile reuses the exchange buffers
     }
@@ -236,17 +224,23 @@ k_ragged_tma(const RaggedEntry* __restrict__ reqs, int nreq, uint64_t totalTiles
 
 namespace backend {
 
-template <int N>
+template <int N, int E>
 static constexpr int raggedSmem() {
-    constexpr int E = raggedE(dev::ilog2c(N));
     return (kRaggedThreads / (N / E)) * dev::smem_stride<N, E, false>() * 8;
 }
 
 static constexpr int maxi(int a, int b) { return a > b ? a : b; }
 
+template <int N>
+static constexpr int raggedSmemBoth() {
+    return maxi(raggedSmem<N, 8>(), raggedSmem<N, 16>());
+}
+
+// Exchange buffer of the largest variant (every kernel serves every variant).
 int raggedSmemBytes() {
-    return maxi(maxi(maxi(raggedSmem<32>(), raggedSmem<64>()), maxi(raggedSmem<128>(), raggedSmem<256>())),
-                maxi(maxi(raggedSmem<512>(), raggedSmem<1024>()), maxi(raggedSmem<2048>(), raggedSmem<4096>())));
+    return maxi(maxi(maxi(raggedSmemBoth<32>(), raggedSmemBoth<64>()), maxi(raggedSmemBoth<128>(), raggedSmemBoth<256>())),
+                maxi(maxi(raggedSmemBoth<512>(), raggedSmemBoth<1024>()),
+                     maxi(raggedSmemBoth<2048>(), raggedSmem<4096, 16>())));
 }
 
 int raggedGrid(int device, int* grid) {

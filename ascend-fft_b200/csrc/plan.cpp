@@ -1392,7 +1392,10 @@ int Ragged::deviceStatus(unsigned* status) {
     return backend::raggedStatus(status, true) ? -6 : 0;
 }
 
-std::unique_ptr<Ragged> Plan::makeRagged(const RaggedRequest* reqs, size_t count, int* status) {
+static_assert(RaggedConfig{}.radix8 == kRaggedDefaultRadix8, "default ragged radices differ");
+
+std::unique_ptr<Ragged> Plan::makeRagged(const RaggedRequest* reqs, size_t count, int* status,
+                                         const RaggedConfig* config) {
     int dummy = 0;
     int& st = status ? *status : dummy;
     st = -8;
@@ -1403,32 +1406,44 @@ std::unique_ptr<Ragged> Plan::makeRagged(const RaggedRequest* reqs, size_t count
             (r.direction != -1 && r.direction != 1))
             return nullptr;
     }
+    bool aligned = true;
+    for (size_t i = 0; i < count; ++i) aligned = aligned && ((uintptr_t)reqs[i].in % 16u) == 0;
+    RaggedConfig cfg;
+    if (config) {
+        cfg = *config;
+        if (cfg.mode < -1 || cfg.mode > 2 || (cfg.mode > 0 && !aligned) ||
+            (cfg.radix8 >> (kRaggedMaxLog - kRaggedMinLog)) != 0)
+            return nullptr;
+    } else {
+        cfg.mode = -1;   // one tile per CTA: measured fastest on B200 (hardware CTA scheduling)
+        if (const char* env = std::getenv("BFLY_RAGGED_STAGES")) {
+            const int want = std::atoi(env);
+            if (want >= -1 && want <= 2) cfg.mode = (aligned || want < 0) ? want : 0;
+        }
+    }
     std::vector<RaggedEntry> es(count);
     uint64_t tile = 0;
     for (size_t i = 0; i < count; ++i) {
         const RaggedRequest& r = reqs[i];
         int logn = 0;
         while ((1u << logn) < r.n) ++logn;
-        const int e = raggedE(logn);
+        const int e = (cfg.radix8 >> (logn - kRaggedMinLog)) & 1u ? 8 : 16;
+        if (!raggedVariant(logn, e)) return nullptr;
         if (prepareC2C(r.n, e)) {
             st = -2;
             return nullptr;
         }
-        const uint32_t rows = raggedRows(logn);
+        const uint32_t rows = raggedRows(logn, e);
         es[i] = RaggedEntry{r.in, r.out, impl_->twC2C[{r.n, e}], r.batch, tile, (uint32_t)logn,
-                            r.direction, r.scale, rows, 0};
+                            r.direction, r.scale, rows, (uint32_t)e, 0};
         tile += (r.batch + rows - 1) / rows;
     }
     std::unique_ptr<Ragged> rg(new Ragged());
     rg->count_ = count;
     rg->total_ = tile;
-    bool aligned = true;
-    for (size_t i = 0; i < count; ++i) aligned = aligned && ((uintptr_t)reqs[i].in % 16u) == 0;
-    rg->stages_ = -1;   // one tile per CTA: measured fastest on B200 (hardware CTA scheduling)
-    if (const char* env = std::getenv("BFLY_RAGGED_STAGES")) {
-        const int want = std::atoi(env);
-        if (want >= -1 && want <= 2) rg->stages_ = (aligned || want < 0) ? want : 0;
-    }
+    rg->stages_ = cfg.mode;
+    rg->radix8_ = cfg.radix8;
+    rg->aligned_ = aligned;
     const int grc = rg->stages_ > 0 ? backend::raggedStagedGrid(impl_->device, rg->stages_, &rg->grid_)
                                     : backend::raggedGrid(impl_->device, &rg->grid_);
     if (grc) {
@@ -1469,6 +1484,29 @@ std::unique_ptr<Ragged> Plan::makeRagged(const RaggedRequest* reqs, size_t count
     }
     st = 0;
     return rg;
+}
+
+double Plan::timeRagged(const Ragged& rg) {
+    if (!impl_) return -1.0;
+    if (!impl_->timer && backend::timerCreate(&impl_->timer)) return -3.0;
+    auto chain = [&](int reps, float* ms) -> int {
+        if (backend::timerStart(impl_->timer, stream_)) return -3;
+        for (int i = 0; i < reps; ++i)
+            if (rg.exec(stream_)) return -5;
+        if (backend::timerStop(impl_->timer, stream_, ms)) return -3;
+        return 0;
+    };
+    float ms = 0.f;
+    if (int r = chain(1, &ms)) return r;   // warm-up
+    if (int r = chain(1, &ms)) return r;
+    const int reps = std::max(1, std::min(64, (int)(1.0 / std::max(ms, 1e-4f))));
+    double best = 0.0;
+    for (int r = 0; r < 3; ++r) {
+        if (int e = chain(reps, &ms)) return e;
+        const double us = ms * 1000.0 / reps;
+        if (r == 0 || us < best) best = us;
+    }
+    return best;
 }
 
 // ================================================================== Context
@@ -1707,6 +1745,186 @@ std::unique_ptr<Plan> Context::select(uint32_t n, uint32_t batch, int topK, std:
         cache.push_back({hw_.gpu, "c2c", best->candidate().id, (long long)n, (long long)batch, bestUs});
         writeCache(tuningCache_, cache);
     }
+    return best;
+}
+
+namespace {
+// Key of a ragged work list's shape: lengths and batch counts in order, and whether every input
+// is 16-byte aligned (the staged modes need it).  Pointers, directions and scales do not change
+// the launch cost and are left out.  FNV-1a, 64 bits.
+uint64_t raggedShapeHash(const RaggedRequest* reqs, size_t count, bool aligned) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        for (int i = 0; i < 8; ++i) {
+            h ^= (v >> (8 * i)) & 0xFFu;
+            h *= 1099511628211ull;
+        }
+    };
+    mix(count);
+    mix(aligned ? 1 : 0);
+    for (size_t i = 0; i < count; ++i) {
+        mix(reqs[i].n);
+        mix(reqs[i].batch);
+    }
+    return h;
+}
+
+std::string raggedCacheId(uint64_t hash, const RaggedConfig& c) {
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), "h%016llx mode %d radix8 0x%02x", (unsigned long long)hash, c.mode,
+                  (unsigned)c.radix8);
+    return buf;
+}
+
+bool parseRaggedCacheId(const std::string& id, uint64_t* hash, RaggedConfig* c) {
+    unsigned long long h = 0;
+    int mode = 0;
+    unsigned mask = 0;
+    if (std::sscanf(id.c_str(), "h%16llx mode %d radix8 0x%x", &h, &mode, &mask) != 3) return false;
+    *hash = h;
+    c->mode = mode;
+    c->radix8 = mask;
+    return true;
+}
+}  // namespace
+
+std::unique_ptr<Ragged> Context::tuneRagged(Plan& plan, const RaggedRequest* reqs, size_t count, int* status,
+                                            std::string* log) {
+    int dummy = 0;
+    int& st = status ? *status : dummy;
+    char line[256];
+    if (log) log->clear();
+    // the default build validates the requests and tells the alignment
+    std::unique_ptr<Ragged> best = plan.makeRagged(reqs, count, &st, nullptr);
+    if (!best) return nullptr;
+    if (best->stages() != -1) {   // an environment override of the mode: start from the default
+        RaggedConfig def;
+        best = plan.makeRagged(reqs, count, &st, &def);
+        if (!best) return nullptr;
+    }
+    const bool aligned = best->aligned();
+    const uint64_t hash = raggedShapeHash(reqs, count, aligned);
+    uint64_t rows = 0;
+    for (size_t i = 0; i < count; ++i) rows += reqs[i].batch;
+
+    std::vector<CacheEntry> cache;
+    if (!tuningCache_.empty()) {
+        cache = readCache(tuningCache_);
+        for (const auto& e : cache) {
+            uint64_t h = 0;
+            RaggedConfig c;
+            if (e.gpu != hw_.gpu || e.kind != "ragged" || e.n != (long long)count || e.batch != (long long)rows ||
+                !parseRaggedCacheId(e.id, &h, &c) || h != hash)
+                continue;
+            int cst = 0;
+            auto rg = plan.makeRagged(reqs, count, &cst, &c);
+            if (rg) {
+                if (log) {
+                    std::snprintf(line, sizeof(line), "selected: mode %d radix8 0x%02x (tuning cache, %.1f us)\n",
+                                  c.mode, (unsigned)c.radix8, e.us);
+                    *log += line;
+                }
+                st = 0;
+                return rg;
+            }
+        }
+    }
+
+    double bestUs = plan.timeRagged(*best);
+    if (bestUs < 0) {
+        st = -5;
+        return nullptr;
+    }
+    if (log) {
+        std::snprintf(line, sizeof(line), "requests=%zu rows=%llu tiles=%llu aligned=%d\n", count,
+                      (unsigned long long)rows, (unsigned long long)best->tiles(), aligned ? 1 : 0);
+        *log += line;
+        std::snprintf(line, sizeof(line), "  mode %2d radix8 0x%02x  %9.2f us  (default)\n", best->stages(),
+                      (unsigned)best->config().radix8, bestUs);
+        *log += line;
+    }
+    // A candidate is timed next to the incumbent in the order candidate, incumbent, incumbent,
+    // candidate and each is the mean of its two timings: the device slows by a few percent
+    // under sustained load, and this order cancels a drift that is linear over the four.
+    // It replaces the incumbent only when >= 1% faster.
+    auto tryConfig = [&](const RaggedConfig& c) -> int {
+        int cst = 0;
+        auto rg = plan.makeRagged(reqs, count, &cst, &c);
+        if (!rg) return cst ? cst : -1;
+        const double a0 = plan.timeRagged(*rg);
+        const double b0 = plan.timeRagged(*best);
+        const double b1 = plan.timeRagged(*best);
+        const double a1 = plan.timeRagged(*rg);
+        if (a0 < 0 || a1 < 0 || b0 < 0 || b1 < 0) return -5;
+        const double us = 0.5 * (a0 + a1);
+        bestUs = 0.5 * (b0 + b1);
+        unsigned dstat = 0;
+        if (c.mode > 0 && (Ragged::deviceStatus(&dstat) || dstat)) {   // a bounded wait gave up
+            if (log) {
+                std::snprintf(line, sizeof(line), "  mode %2d radix8 0x%02x  rejected (device status %u)\n",
+                              c.mode, (unsigned)c.radix8, dstat);
+                *log += line;
+            }
+            return 0;
+        }
+        const bool better = us < bestUs * 0.99;
+        if (log) {
+            std::snprintf(line, sizeof(line), "  mode %2d radix8 0x%02x  %9.2f us  (incumbent %.2f us)%s\n", c.mode,
+                          (unsigned)c.radix8, us, bestUs, better ? "  <- best" : "");
+            *log += line;
+        }
+        if (better) {
+            best = std::move(rg);
+            bestUs = us;
+        }
+        return 0;
+    };
+    // lengths present, largest share of points first
+    uint64_t points[kRaggedMaxLog + 1] = {};
+    for (size_t i = 0; i < count; ++i) {
+        int logn = 0;
+        while ((1u << logn) < reqs[i].n) ++logn;
+        points[logn] += reqs[i].batch * reqs[i].n;
+    }
+    std::vector<int> lengths;
+    for (int l = kRaggedMinLog; l <= kRaggedMaxLog; ++l)
+        if (points[l] && raggedVariant(l, 8)) lengths.push_back(l);
+    std::stable_sort(lengths.begin(), lengths.end(), [&](int a, int b) { return points[a] > points[b]; });
+    for (int l : lengths) {
+        RaggedConfig c = best->config();
+        c.radix8 ^= 1u << (l - kRaggedMinLog);
+        if (int r = tryConfig(c)) {
+            st = r;
+            return nullptr;
+        }
+    }
+    for (int mode : {0, 1, 2}) {
+        if (mode > 0 && !aligned) continue;
+        RaggedConfig c = best->config();
+        if (c.mode == mode) continue;
+        c.mode = mode;
+        if (int r = tryConfig(c)) {
+            st = r;
+            return nullptr;
+        }
+    }
+    if (log) {
+        std::snprintf(line, sizeof(line), "selected: mode %d radix8 0x%02x  %.2f us\n", best->stages(),
+                      (unsigned)best->config().radix8, bestUs);
+        *log += line;
+    }
+    if (!tuningCache_.empty()) {
+        cache.erase(std::remove_if(cache.begin(), cache.end(), [&](const CacheEntry& e) {
+                        uint64_t h = 0;
+                        RaggedConfig c;
+                        return e.gpu == hw_.gpu && e.kind == "ragged" && e.n == (long long)count &&
+                               e.batch == (long long)rows && parseRaggedCacheId(e.id, &h, &c) && h == hash;
+                    }), cache.end());
+        cache.push_back({hw_.gpu, "ragged", raggedCacheId(hash, best->config()), (long long)count, (long long)rows,
+                         bestUs});
+        writeCache(tuningCache_, cache);
+    }
+    st = 0;
     return best;
 }
 

@@ -144,6 +144,15 @@ struct RaggedRequest {
     float scale;
 };
 
+// How a ragged work list is launched: the launch mode (see Ragged::stages) and, per length,
+// the register radix of its tiles -- bit (log2 n - 5) of radix8 set: 256 threads x 8 values
+// (2048 points) per tile, else x 16 (4096 points); n = 4096 has only the 16-value tiles, so
+// bit 7 must be clear.  The default is the library's measured choice for a typical mix.
+struct RaggedConfig {
+    int mode = -1;
+    uint32_t radix8 = 0x3;   // n = 32 and 64 with 8 values per thread
+};
+
 // A device work list for one persistent launch over many requests of different lengths and
 // batch counts (built once; exec() is a single kernel launch, capturable in a CUDA graph).
 // Must not outlive the Plan that built it (it uses that plan's twiddle tables).
@@ -158,6 +167,10 @@ public:
     // with plain loads; 1 or 2 persistent CTAs with tiles staged in shared memory by bulk copies
     // (all inputs 16-byte aligned).  The environment variable BFLY_RAGGED_STAGES overrides.
     int stages() const { return stages_; }
+    // The launch mode and per-length radices this work list was built with.
+    RaggedConfig config() const { return RaggedConfig{stages_, radix8_}; }
+    // True when every input is 16-byte aligned (the staged modes need it).
+    bool aligned() const { return aligned_; }
     // Device status of staged launches: 0, or 1 when a bounded wait ran out (then cleared).
     static int deviceStatus(unsigned* status);
 
@@ -170,6 +183,8 @@ private:
     uint64_t total_ = 0;
     int grid_ = 0;
     int stages_ = 0;
+    uint32_t radix8_ = 0;
+    bool aligned_ = false;
 };
 
 class Plan {
@@ -275,8 +290,15 @@ public:
     static int longStatus(unsigned* status);   // cluster long-C2C kernel, same convention
 
     // Build a ragged persistent launch over `count` requests; *status receives 0 or a code
-    // (-8 invalid request, -2 table build, -3 alloc, -4 upload, -1 runtime).
-    std::unique_ptr<Ragged> makeRagged(const RaggedRequest* reqs, size_t count, int* status);
+    // (-8 invalid request or configuration, -2 table build, -3 alloc, -4 upload, -1 runtime).
+    // Without `config` the default applies (BFLY_RAGGED_STAGES=-1/0/1/2 overrides its mode);
+    // a staged mode (1, 2) with an input that is not 16-byte aligned is invalid.
+    std::unique_ptr<Ragged> makeRagged(const RaggedRequest* reqs, size_t count, int* status,
+                                       const RaggedConfig* config = nullptr);
+    // Device time of one launch of `rg` (CUDA events on the plan stream around chains of
+    // back-to-back launches of ~1 ms, best of 3), or a negative code.  Runs the work list:
+    // every output -- and an in-place request's input -- is overwritten.
+    double timeRagged(const Ragged& rg);
 
     void* stream() const { return stream_; }
 
@@ -333,6 +355,17 @@ public:
     std::unique_ptr<Plan> select(uint32_t n, uint32_t batch, int topK = 3,
                                  std::string* log = nullptr);
     std::unique_ptr<Plan> makePlan(const Candidate& c);
+    // Autotuner of the ragged launch: build the work list on `plan` with the default
+    // configuration, then measure the other register radix of each length present (largest
+    // share of points first) and the other launch modes, each timed next to the incumbent
+    // (candidate, incumbent, incumbent, candidate) and kept only when the whole list runs >= 1%
+    // faster; returns the fastest.  Executes the list many times
+    // (outputs, and in-place inputs, are overwritten).  With a tuning cache set, a cached choice
+    // for the same lengths, batch counts and input alignment on this GPU is built without
+    // measuring, and new choices are persisted.  *status as Plan::makeRagged, -5 when a launch
+    // or a timing fails.
+    std::unique_ptr<Ragged> tuneRagged(Plan& plan, const RaggedRequest* reqs, size_t count,
+                                       int* status, std::string* log = nullptr);
     // Persist autotuned choices in a JSON file; "" disables.
     void setTuningCache(const std::string& path) { tuningCache_ = path; }
     void* stream() const;

@@ -250,6 +250,24 @@ int bfly_ragged_info(bfly_ragged* ragged, uint64_t* tiles, int* grid, int* stage
 /* Status word of the staged launches on the current device: 0, or 1 when a bounded wait for a
  * staged copy ran out (the launch then stopped early); reading clears it. */
 int bfly_ragged_device_status(unsigned* status);
+/* The same work list built with an explicit launch configuration: mode as above (-1, 0, 1, 2;
+ * 1 and 2 need every input 16-byte aligned) and, per length, the register radix of its tiles:
+ * bit (log2 n - 5) of radix8 set = 256 threads x 8 values per tile, clear = x 16 (n = 4096 has
+ * only the 16-value tiles, so bit 7 must be clear).  bfly_ragged_create uses mode -1 and
+ * radix8 = 0x3.  -8 for an invalid request or configuration. */
+int bfly_ragged_create_config(bfly_plan* plan, const bfly_ragged_request* reqs, size_t count, int mode,
+                              uint32_t radix8, bfly_ragged** out);
+/* Autotuned work list (the ragged counterpart of bfly_context_select): builds the default
+ * configuration, then measures the other radix of each length present and the other launch
+ * modes on these very requests, and returns the fastest.  It runs the list many times: outputs
+ * (and the inputs of in-place requests) are overwritten.  With a tuning cache set, the choice
+ * for the same lengths, batch counts and input alignment on this GPU is reused without
+ * measuring.  log may be NULL.  Returns 0, a bfly_ragged_create code, or -5 when a launch or
+ * timing failed. */
+int bfly_context_tune_ragged(bfly_context* ctx, bfly_plan* plan, const bfly_ragged_request* reqs, size_t count,
+                             bfly_ragged** out, char* log, size_t log_cap);
+/* Launch mode and radix mask of a work list. */
+int bfly_ragged_config(bfly_ragged* ragged, int* mode, uint32_t* radix8);
 void bfly_ragged_destroy(bfly_ragged* ragged);
 
 /* New: long C2C (four-step, n in {8192, 16384, 32768, 65536}) that allocates no device memory,

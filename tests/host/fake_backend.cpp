@@ -18,6 +18,8 @@ int streamsCreated = 0, streamsDestroyed = 0;
 int deviceCountValue = 1;
 bool pageableHost = false;   // report host buffers as pageable (staged round trips)
 float timerMs = 0.01f;   // reported time per launch
+int timedExtra = 0;       // extra launch-equivalents of time, added by costed fake kernels
+int raggedCost16 = 0;     // time of a ragged launch: + this many launches per 16-value request
 }  // namespace fake
 
 namespace bfly {
@@ -92,9 +94,9 @@ int streamSync(void*) {
 // Elapsed time: timerMs per kernel launched between start and stop (at least one).
 struct Timer { int launchesAtStart; };
 int timerCreate(Timer** t) { *t = new Timer{0}; return 0; }
-int timerStart(Timer* t, void*) { t->launchesAtStart = fake::launches; return 0; }
+int timerStart(Timer* t, void*) { t->launchesAtStart = fake::launches + fake::timedExtra; return 0; }
 int timerStop(Timer* t, void*, float* ms) {
-    const int k = fake::launches - t->launchesAtStart;
+    const int k = fake::launches + fake::timedExtra - t->launchesAtStart;
     *ms = fake::timerMs * (float)(k > 1 ? k : 1);
     return 0;
 }
@@ -463,6 +465,7 @@ int launchRagged(const void* entries, int count, uint64_t, int, void*) {
     if (int r = launch()) return r;
     const RaggedEntry* es = static_cast<const RaggedEntry*>(entries);
     for (int i = 0; i < count; ++i) {
+        if (es[i].e == 16) fake::timedExtra += fake::raggedCost16;
         const uint32_t n = 1u << es[i].logn;
         for (uint64_t b = 0; b < es[i].batch; ++b)
             dft((const float*)es[i].in + b * 2 * n, (float*)es[i].out + b * 2 * n, n, es[i].direction,

@@ -25,6 +25,7 @@ extern int allocations, releases, copies, launches, syncs;
 extern int failAllocation, failCopy, failLaunch, failSync;
 extern int streamsCreated, streamsDestroyed, deviceCountValue;
 extern float timerMs;
+extern int timedExtra, raggedCost16;
 extern bool pageableHost;
 }  // namespace fake
 
@@ -364,6 +365,50 @@ int main(int argc, char** argv) {
         fake::failAllocation = fake::allocations + 1;
         CHECK(!plan->makeRagged(ok, 2, &st) && st == -3);
         fake::failAllocation = 0;
+
+        // explicit configurations: the radix sets the rows per tile, invalid ones are refused
+        std::vector<float> c(2 * 128 * 20), oc(c.size());
+        for (size_t i = 0; i < c.size(); ++i) c[i] = bfly::patternAt(i + 11);
+        bfly::RaggedRequest mix[] = {{a.data(), oa.data(), 64, 3, -1, 1.f}, {c.data(), oc.data(), 128, 20, -1, 1.f}};
+        bfly::RaggedConfig all8{-1, 0x7F}, all16{-1, 0x0};
+        auto r8 = plan->makeRagged(mix, 2, &st, &all8);
+        CHECK(r8 && st == 0 && r8->tiles() == 1 + 2);   // 64: 32 rows per tile; 128: 16 rows per tile
+        CHECK(r8->config().radix8 == 0x7F && r8->config().mode == -1);
+        CHECK(r8->exec(nullptr) == 0);
+        bfly::refFftF32(c.data() + 19 * 256, r.data(), 128);
+        CHECK(bfly::maxRelScaled(oc.data() + 19 * 256, r.data(), 256) < 1e-5);
+        auto r16 = plan->makeRagged(mix, 2, &st, &all16);
+        CHECK(r16 && r16->tiles() == 1 + 1);            // 64: 64 rows per tile; 128: 32 rows per tile
+        const int allocBad = fake::allocations;
+        bfly::RaggedConfig bad4096{-1, 0x80}, badMode{3, 0x3}, staged{1, 0x3};
+        CHECK(!plan->makeRagged(mix, 2, &st, &bad4096) && st == -8);
+        CHECK(!plan->makeRagged(mix, 2, &st, &badMode) && st == -8);
+        bfly::RaggedRequest odd[] = {{c.data() + 2, oc.data(), 64, 1, -1, 1.f}};   // 8-byte aligned input
+        CHECK(!plan->makeRagged(odd, 1, &st, &staged) && st == -8);
+        CHECK(fake::allocations == allocBad);
+        auto rs = plan->makeRagged(mix, 2, &st, &staged);
+        CHECK(rs && rs->stages() == 1 && rs->aligned());
+
+        // autotuner: 16-value tiles made slower by the fake timer, so both lengths present move
+        // to 8 values; the modes cost the same and stay at the default; the choice is persisted
+        // and reused without measuring
+        fake::raggedCost16 = 4;
+        std::string tlog;
+        auto tuned = context.tuneRagged(*plan, ok, 2, &st, &tlog);
+        CHECK(tuned && st == 0);
+        CHECK(tuned->config().radix8 == 0x7 && tuned->config().mode == -1);
+        CHECK(tlog.find("selected: mode -1 radix8 0x07") != std::string::npos);
+        CHECK(read(cache).find("\"kind\": \"ragged\"") != std::string::npos);
+        const int launchesTuned = fake::launches;
+        std::string tlog2;
+        auto again = context.tuneRagged(*plan, ok, 2, &st, &tlog2);
+        CHECK(again && again->config().radix8 == 0x7 && tlog2.find("tuning cache") != std::string::npos);
+        CHECK(fake::launches == launchesTuned);
+        bfly::RaggedRequest other[] = {{a.data(), oa.data(), 64, 2, -1, 1.f}};   // another shape: measured
+        auto t3 = context.tuneRagged(*plan, other, 1, &st, nullptr);
+        CHECK(t3 && t3->config().radix8 == 0x3 && fake::launches > launchesTuned);
+        CHECK(!context.tuneRagged(*plan, bad, 1, &st, nullptr) && st == -8);
+        fake::raggedCost16 = 0;
     }
 
     {   // 2-D and middle-axis transforms: exact against a direct FP64 DFT of the same layout
