@@ -296,7 +296,8 @@ public:
     std::unique_ptr<Ragged> makeRagged(const RaggedRequest* reqs, size_t count, int* status,
                                        const RaggedConfig* config = nullptr);
     // Device time of one launch of `rg` (CUDA events on the plan stream around chains of
-    // back-to-back launches of ~1 ms, best of 3), or a negative code.  Runs the work list:
+    // back-to-back launches of ~1 ms, best of 3, after ~3 ms of untimed launches), or a
+    // negative code.  Runs the work list:
     // every output -- and an in-place request's input -- is overwritten.
     double timeRagged(const Ragged& rg);
 
@@ -359,7 +360,7 @@ public:
     // configuration, then measure the other register radix of each length present (largest
     // share of points first) and the other launch modes, each timed next to the incumbent
     // (candidate, incumbent, incumbent, candidate) and kept only when the whole list runs >= 1%
-    // faster; returns the fastest.  Executes the list many times
+    // faster in two such comparisons; returns the fastest.  Executes the list many times
     // (outputs, and in-place inputs, are overwritten).  With a tuning cache set, a cached choice
     // for the same lengths, batch counts and input alignment on this GPU is built without
     // measuring, and new choices are persisted.  *status as Plan::makeRagged, -5 when a launch
