@@ -54,7 +54,7 @@ def test_every_mixed_length(plan, cuda):
 
 
 @pytest.mark.parametrize("n", [6, 60, 100, 360, 1000, 2401, 3000, 5000, 6561, 10935, 12000, 12250, 11, 143, 1001,
-                               4095, 1331, 2197, 9152])
+                               4095, 1331, 2197, 9152, 441, 882, 1764, 2205, 3600])
 @pytest.mark.parametrize("direction", [-1, 1])
 def test_mixed_large_batches(plan, cuda, n, direction):
     """Many rows per launch, batch not a multiple of the rows per CTA."""
