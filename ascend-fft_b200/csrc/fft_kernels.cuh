@@ -48,7 +48,7 @@ k_c2c(const float2* __restrict__ in, float2* __restrict__ out, const float2* __r
     float2* dst = out + row * N;
     float2 v[E];
     TM::run(v, smem + rl * S, tw, t, rl,
-            [&](int i) { return ok ? ld_stream(src + i) : make_float2(0.f, 0.f); });
+            [&](int i) { return ok ? ld_once_ca(src + i) : make_float2(0.f, 0.f); });
     pdl_trigger();
     if (ok) TM::for_each_out(v, t, [&](int i, float2 x) { st_stream(dst + i, cscale(x, scale)); });
 }

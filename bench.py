@@ -957,7 +957,7 @@ def run_ours(args):
         "per_point_graph": {"value": round(per_point_gbs, 1), "launches_per_step": len(pts)},
         "largest_launch": {"kernel": "k_c2c N=4096 batch=4096",
                            "frac": round(dom_bytes / (dom_ms / 1e3) / 1e9 / peak, 4),
-                           "launch_us": round(dom_ms * 1e3, 2), "l2": "134 MB in, near the L2: partly warm"},
+                           "launch_us": round(dom_ms * 1e3, 2), "l2": "134 MB in, about the L2 size"},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d, "path": "bfly_plan_run_c2c_many, pinned host buffers",
                 "scopes": scopes},
