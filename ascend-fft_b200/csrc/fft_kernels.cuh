@@ -217,7 +217,7 @@ k_long_a(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
     float2* dst = out + b * N + n2;
     (void)batch;
     float2 v[E];
-    TM::run(v, smem + c * S, tw, t, 0, [&](int i) { return ld_stream(src + ((size_t)i << logN2)); });
+    TM::run(v, smem + c * S, tw, t, 0, [&](int i) { return ld_once_ca(src + ((size_t)i << logN2)); });
     TM::for_each_out(v, t, [&](int k1, float2 x) {
         const uint32_t m = n2 * (uint32_t)k1;
         const float2 w = cmul<false>(__ldg(thi + (m >> 8)), __ldg(tlo + (m & 255u)));
@@ -246,7 +246,7 @@ k_long_b(const float2* __restrict__ in, float2* __restrict__ out, const float2* 
     float2* sm = smem + rl * S;
     (void)batch;
     float2 v[E];
-    TM::run(v, sm, tw, t, rl, [&](int i) { return ld_stream(src + i); });
+    TM::run(v, sm, tw, t, rl, [&](int i) { return ld_once_ca(src + i); });
     __syncthreads();
     TM::for_each_out(v, t, [&](int i, float2 x) { sm[spad(i)] = x; });
     __syncthreads();
