@@ -344,7 +344,8 @@ __device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p);
 // (n = 4096: 0.846 -> 0.861 of the copy peak at batch 4096, 0.896 -> 0.914 at 8192), level
 // with read-only (.nc) loads, which are not used because an input may be written by a kernel
 // still draining when this one launches.  The two four-step passes gained too (long C2C
-// n = 32768: 0.433 -> 0.455; 65536: 0.443 -> 0.446); R2C / C2R measured level.  Kernels that
+// n = 32768: 0.433 -> 0.455; 65536: 0.443 -> 0.446) and so did the column pass (NY = 1024:
+// 0.57 -> 0.59); R2C, C2R, the mixed-radix, prime-factor, STFT and Bluestein kernels measured level.  Kernels that
 // keep several twiddle tables in L1 (the ragged launch over many lengths) lost with it and keep
 // ld_stream.
 __device__ __forceinline__ float2 ld_once_ca(const float2* p) { return __ldca(p); }

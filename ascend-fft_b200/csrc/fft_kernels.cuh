@@ -186,7 +186,7 @@ k_cols(const float2* __restrict__ in, float2* __restrict__ out, const float2* __
     float2* dst = out + m * matStride + col;
     float2 v[E];
     TM::run(v, smem + c * S, tw, t, 0, [&](int i) {
-        return live ? ld_stream(src + (size_t)i * pitch) : make_float2(0.f, 0.f);
+        return live ? ld_once_ca(src + (size_t)i * pitch) : make_float2(0.f, 0.f);
     });
     if (live) TM::for_each_out(v, t, [&](int k, float2 x) { st_stream(dst + (size_t)k * pitch, cscale(x, scale)); });
 }
