@@ -975,7 +975,7 @@ def run_case(spec: str, reps: int):
     """Launch one kernel configuration `reps` times without timing (for ncu captures):
     spec = kind:n:batch with kind in c2c, c2c_inv (any n: non-powers of two run the prime-factor, mixed-radix or Bluestein
     kernel), tc2, tc3 (tensor-core splits), r2c, c2r, cluster (long C2C on the cluster
-    schedule), or ragged:grid:CAP; or cols:NY:NCOLS:MATS (column kernel), c2d:NY:NX:B (2-D),
+    schedule), or ragged:grid:CAP or ragged:N:B; or cols:NY:NCOLS:MATS (column kernel), c2d:NY:NX:B (2-D),
     stft:N:HOP:LEN (4 signals, centred, Hann window), istft:N:HOP:LEN (its inverse)."""
     import torch
     import bfly
@@ -1017,14 +1017,13 @@ def run_case(spec: str, reps: int):
     n, b = parts[1], parts[2]
     if kind == "cluster":
         plan = ctx.make_plan("r16_cta256_shared_fp32_cluster", 8192, 1)
-    if kind == "ragged":   # ragged:grid:CAP -> the 49-point grid with batch capped at CAP
-        cap = int(b)
-        bufs = []
-        for nn in GRID_N:
-            for bb in GRID_B:
-                bb = min(bb, cap)
-                x = torch.randn(bb, nn, dtype=torch.complex64, device=dev)
-                bufs.append((x, torch.empty_like(x), nn, bb))
+    if kind == "ragged":   # ragged:grid:CAP -> the 49-point grid with batch capped at CAP;
+        bufs = []          # ragged:N:B -> one request of B rows of length N
+        shapes = ([(nn, min(bb, int(b))) for nn in GRID_N for bb in GRID_B] if n == "grid"
+                  else [(int(n), int(b))])
+        for nn, bb in shapes:
+            x = torch.randn(bb, nn, dtype=torch.complex64, device=dev)
+            bufs.append((x, torch.empty_like(x), nn, bb))
         rg = plan.make_ragged((x.data_ptr(), y.data_ptr(), nn, bb, -1, 1.0) for x, y, nn, bb in bufs)
         for _ in range(reps):
             r = rg.exec(0)
