@@ -20,6 +20,7 @@ bool pageableHost = false;   // report host buffers as pageable (staged round tr
 float timerMs = 0.01f;   // reported time per launch
 int timedExtra = 0;       // extra launch-equivalents of time, added by costed fake kernels
 int raggedCost16 = 0;     // time of a ragged launch: + this many launches per 16-value request
+std::vector<const void*> h2dSources;   // source pointer of every host-to-device copy, in issue order
 }  // namespace fake
 
 namespace bfly {
@@ -79,13 +80,17 @@ int alloc(void** p, size_t bytes) {
 int release(void* p) { ++fake::releases; std::free(p); return 0; }
 int allocHost(void** p, size_t bytes) { *p = std::malloc(bytes); return *p ? 0 : 2; }
 int releaseHost(void* p) { std::free(p); return 0; }
-int copyH2D(void* dst, const void* src, size_t bytes, void*) {
+static int copyBytes(void* dst, const void* src, size_t bytes) {
     ++fake::copies;
     if (fake::copies == fake::failCopy || !dst || !src) return 1;
     std::memcpy(dst, src, bytes);
     return 0;
 }
-int copyD2H(void* dst, const void* src, size_t bytes, void* s) { return copyH2D(dst, src, bytes, s); }
+int copyH2D(void* dst, const void* src, size_t bytes, void*) {
+    fake::h2dSources.push_back(src);
+    return copyBytes(dst, src, bytes);
+}
+int copyD2H(void* dst, const void* src, size_t bytes, void*) { return copyBytes(dst, src, bytes); }
 int streamSync(void*) {
     ++fake::syncs;
     return fake::syncs == fake::failSync ? 1 : 0;

@@ -27,6 +27,7 @@ extern int streamsCreated, streamsDestroyed, deviceCountValue;
 extern float timerMs;
 extern int timedExtra, raggedCost16;
 extern bool pageableHost;
+extern std::vector<const void*> h2dSources;
 }  // namespace fake
 
 #define CHECK(cond)                                                                    \
@@ -699,6 +700,34 @@ int main(int argc, char** argv) {
         const bfly::HostRequest bad4[] = {reqs[0], {a.data(), oa.data(), 64, 0, -1, 1.f}};
         for (const auto* bad : {bad1, bad2, bad3, bad4}) CHECK(plan->runMany(bad, 2) == -8);
         CHECK(fake::allocations == allocBefore && fake::copies == copiesBefore && fake::launches == launchBefore);
+    }
+
+    {   // batched host round trip issue order: every request under 1 MB is uploaded before any
+        // byte of a larger one, whatever the order the caller lists them in
+        std::vector<float> big(2 * 1024 * 160), s1(2 * 64 * 3), s2(2 * 128 * 5);   // 1.25 MB, 1.5 KB, 5 KB
+        for (size_t i = 0; i < big.size(); ++i) big[i] = (float)std::sin(0.01 * i);
+        for (size_t i = 0; i < s1.size(); ++i) s1[i] = (float)std::cos(0.3 * i);
+        for (size_t i = 0; i < s2.size(); ++i) s2[i] = (float)std::sin(0.7 * i + 2);
+        std::vector<float> ob(big.size()), o1(s1.size()), o2(s2.size()), rb(big.size()), r1(s1.size()), r2(s2.size());
+        const bfly::HostRequest reqs[] = {{big.data(), ob.data(), 1024, 160, -1, 1.f},
+                                          {s1.data(), o1.data(), 64, 3, -1, 1.f},
+                                          {s2.data(), o2.data(), 128, 5, 1, 0.5f}};
+        fake::h2dSources.clear();
+        CHECK(plan->runMany(reqs, 3) == 0);
+        auto inside = [](const void* p, const std::vector<float>& v) {
+            return p >= (const void*)v.data() && p < (const void*)(v.data() + v.size());
+        };
+        size_t firstBig = fake::h2dSources.size(), lastSmall = 0, smallSeen = 0;
+        for (size_t i = 0; i < fake::h2dSources.size(); ++i) {
+            const void* p = fake::h2dSources[i];
+            if (inside(p, big)) firstBig = std::min(firstBig, i);
+            if (inside(p, s1) || inside(p, s2)) { lastSmall = i; ++smallSeen; }
+        }
+        CHECK(smallSeen == 2 && firstBig < fake::h2dSources.size() && lastSmall < firstBig);
+        CHECK(plan->execC2C(big.data(), rb.data(), 1024, 160, -1, 1.f, nullptr) == 0);
+        CHECK(plan->execC2C(s1.data(), r1.data(), 64, 3, -1, 1.f, nullptr) == 0);
+        CHECK(plan->execC2C(s2.data(), r2.data(), 128, 5, 1, 0.5f, nullptr) == 0);
+        CHECK(ob == rb && o1 == r1 && o2 == r2);
     }
 
     {   // pageable host buffers go through pinned staging slots: same results as the direct path
